@@ -1,0 +1,76 @@
+/*
+ * Launchers of the sm_100a kernels, callable from the C API layer.  All take
+ * device pointers and a stream and return cudaError_t values as int.
+ */
+#ifndef SG_KERNELS_H
+#define SG_KERNELS_H
+
+#include <stdint.h>
+
+#include "sg_layout.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Per-dim sweep tables as the kernels read them. */
+typedef struct sg_sweep_tables {
+    const sg_chain *chains; /* device */
+    const uint32_t *seg;    /* device */
+    int64_t nchains;
+    int lmax_max;           /* highest lmax over the chains          */
+    int64_t cap32;          /* shared-memory elements for one chain (FP32) */
+    int64_t cap64;          /* same for FP64                          */
+} sg_sweep_tables;
+
+/* Shared-memory bytes a chain-sweep CTA needs, or a negative value if the
+ * chains of this grid do not fit and the per-level gather path must run. */
+int64_t sgk_chain_smem_bytes(int64_t cap_elems, int elem_bytes);
+
+/* One sweep of dim k over all chains, FP32 in place, staged through shared
+ * memory with bulk copies.  err: device int, set nonzero on a wait timeout. */
+int sgk_sweep_chains_f32(float *a, const sg_sweep_tables *t, int *err, void *stream);
+int sgk_sweep_chains_f64(double *a, const sg_sweep_tables *t, int *err, void *stream);
+/* The same sweep as lmax_max launches, finest level first, gathering the
+ * parents from global memory (any chain size). */
+int sgk_sweep_gather_f32(float *a, const sg_sweep_tables *t, void *stream);
+int sgk_sweep_gather_f64(double *a, const sg_sweep_tables *t, void *stream);
+int sgk_widen(const float *src, double *dst, int64_t n, void *stream);
+int sgk_narrow(const double *src, float *dst, int64_t n, void *stream);
+
+/* Evaluation. */
+typedef struct sg_eval_plan {
+    const float *alpha;     /* device grid, group-aligned layout             */
+    const uint32_t *leaf;   /* device: subspace offsets in depth-first order */
+    int d, n;
+    int lim[SG_MAX_DIMS];
+    int ppt;                /* points per thread (1 or 2)                    */
+} sg_eval_plan;
+
+/* out[perm ? perm[i] : i] = interpolant at coords[i*d .. i*d+d-1]. */
+int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm,
+                 float *out, int64_t num_evals, void *stream);
+
+/* Spatial ordering of query points: writes the sorted coordinates and the
+ * permutation (sorted position -> caller position).  scratch: device bytes
+ * of at least sgk_sort_scratch_bytes(num_evals, d). */
+int64_t sgk_sort_scratch_bytes(int64_t num_evals, int d);
+int sgk_sort_points(const float *coords, int64_t num_evals, int d, void *scratch,
+                    float *sorted, int32_t *perm, void *stream);
+
+/* Batched bijection on the device. */
+int sgk_idx2gp(const sg_layout *L, const int64_t *index, int *levels, int *indices,
+               int64_t count, void *stream);
+int sgk_gp2idx(const sg_layout *L, const int *levels, const int *indices, int64_t *index,
+               int64_t count, void *stream);
+
+/* f at every point of the device grid (group-aligned layout), FP64 -> FP32. */
+int sgk_sample(const sg_layout *L, int fn, const double *params, int nparams, float *alpha,
+               void *stream);
+
+int sgk_num_sms(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,243 @@
+/*
+ * Host-side index algebra (C).  Follows the reference benchmark
+ * adaptive_sparse_grid_bench.c: tables c:101-140 (with the limit handling of
+ * the CUDA host code, adaptive_sparse_grid_bench_cuda.cu:79-102), bijection
+ * c:187-279.  Also builds the per-sweep chain tables and the evaluation
+ * order table that the kernels walk.
+ */
+#include "sg_layout.h"
+
+#include <stdlib.h>
+#include <string.h>
+
+int sg_layout_init(sg_layout *L, int d, int n, const int *limits)
+{
+    int i, s, k;
+    if (!L || d < 1 || n < 1) return SG_ERR_ARG;
+    if (d > SG_MAX_DIMS || n > SG_MAX_LEVELS) return SG_ERR_RANGE;
+    memset(L, 0, sizeof(*L));
+    L->d = d;
+    L->n = n;
+    for (i = 0; i < d; i++) {
+        int v = limits ? limits[i] : n - 1;
+        if (v < 0) return SG_ERR_ARG;
+        L->lim[i] = v > n - 1 ? n - 1 : v;
+    }
+    /* dp[i][s] = sum_{k <= min(s, lim_i)} dp[i-1][s-k]  (c:113-129) */
+    for (s = 0; s < n; s++) L->dp[0][s] = s <= L->lim[0];
+    for (i = 1; i < d; i++)
+        for (s = 0; s < n; s++) {
+            int64_t c = 0;
+            for (k = 0; k <= s && k <= L->lim[i]; k++) c += L->dp[i - 1][s - k];
+            L->dp[i][s] = c;
+        }
+    /* group offsets (c:132-140), compact and padded */
+    L->N = L->S = L->Npad = 0;
+    for (s = 0; s < n; s++) {
+        int64_t sz = L->dp[d - 1][s] << s;
+        L->lidx[s] = L->N;
+        L->plidx[s] = L->Npad;
+        L->N += sz;
+        L->S += L->dp[d - 1][s];
+        L->Npad += (sz + SG_GROUP_ALIGN - 1) / SG_GROUP_ALIGN * SG_GROUP_ALIGN;
+    }
+    L->lidx[n] = L->N;
+    L->plidx[n] = L->Npad;
+    /* kernels index the device grid with 32-bit offsets */
+    if (L->Npad >= ((int64_t)1 << 31)) return SG_ERR_RANGE;
+    return SG_OK;
+}
+
+/* c:266-279 */
+int64_t sg_layout_l2idx(const sg_layout *L, const int *lv)
+{
+    int64_t pos = 0;
+    int i, j, sum = lv[0];
+    for (i = 1; i < L->d; i++) {
+        sum += lv[i];
+        for (j = 0; j < lv[i]; j++) pos += L->dp[i - 1][sum - j];
+    }
+    return pos;
+}
+
+/* c:245-264 */
+void sg_layout_idx2l(const sg_layout *L, int64_t pos, int s, int *lv)
+{
+    int i;
+    for (i = L->d - 1; i >= 1; i--) {
+        int level = 0;
+        while (pos >= L->dp[i - 1][s - level]) {
+            pos -= L->dp[i - 1][s - level];
+            level++;
+        }
+        lv[i] = level;
+        s -= level;
+    }
+    lv[0] = s;
+}
+
+/* c:187-207 */
+int64_t sg_layout_gp2idx(const sg_layout *L, const int *lv, const int *ix)
+{
+    int64_t in_sub = ix[0];
+    int i, s = lv[0];
+    for (i = 1; i < L->d; i++) {
+        in_sub = (in_sub << lv[i]) + ix[i];
+        s += lv[i];
+    }
+    return L->lidx[s] + (sg_layout_l2idx(L, lv) << s) + in_sub;
+}
+
+/* c:210-243 */
+int sg_layout_idx2gp(const sg_layout *L, int64_t idx, int *lv, int *ix)
+{
+    int s = 0, i;
+    int64_t rest;
+    if (idx < 0 || idx >= L->N) return SG_ERR_ARG;
+    while (s < L->n && idx >= L->lidx[s]) s++;
+    s--;
+    idx -= L->lidx[s];
+    rest = idx & (((int64_t)1 << s) - 1);
+    sg_layout_idx2l(L, idx >> s, s, lv);
+    for (i = L->d - 1; i >= 0; i--) {
+        ix[i] = (int)(rest & (((int64_t)1 << lv[i]) - 1));
+        rest >>= lv[i];
+    }
+    return SG_OK;
+}
+
+int64_t sg_layout_subspace_offset(const sg_layout *L, const int *lv)
+{
+    int i, s = 0;
+    for (i = 0; i < L->d; i++) s += lv[i];
+    return L->plidx[s] + (sg_layout_l2idx(L, lv) << s);
+}
+
+/* Odometer over level vectors of the dims in `dims` (count m) with sum <= cap
+ * and per-dim limits; calls back with the vector written into lv. */
+typedef void (*lv_visit)(void *ctx, int *lv, int sum);
+
+static void enum_levels(const sg_layout *L, const int *dims, int m, int idx, int cap,
+                        int sum, int *lv, lv_visit fn, void *ctx)
+{
+    int l, k;
+    if (idx == m) {
+        fn(ctx, lv, sum);
+        return;
+    }
+    k = dims[idx];
+    for (l = 0; l <= L->lim[k] && sum + l <= cap; l++) {
+        lv[k] = l;
+        enum_levels(L, dims, m, idx + 1, cap, sum + l, lv, fn, ctx);
+    }
+    lv[k] = 0;
+}
+
+typedef struct {
+    const sg_layout *L;
+    int k;
+    sg_chain *chains;
+    int64_t nch, cap_ch;
+    uint32_t *seg;
+    int64_t nseg, cap_seg;
+    int err;
+} chain_ctx;
+
+static void chain_visit(void *vctx, int *lv, int sigma)
+{
+    chain_ctx *c = (chain_ctx *)vctx;
+    const sg_layout *L = c->L;
+    int k = c->k, j, m, lo = 0;
+    int lmax = L->n - 1 - sigma;
+    if (lmax > L->lim[k]) lmax = L->lim[k];
+    if (lmax < 1 || c->err) return;
+    if (c->nch == c->cap_ch) {
+        c->cap_ch = c->cap_ch ? 2 * c->cap_ch : 1024;
+        c->chains = (sg_chain *)realloc(c->chains, (size_t)c->cap_ch * sizeof(sg_chain));
+        if (!c->chains) { c->err = SG_ERR_NOMEM; return; }
+    }
+    while (c->nseg + lmax + 1 > c->cap_seg) {
+        c->cap_seg = c->cap_seg ? 2 * c->cap_seg : 4096;
+        c->seg = (uint32_t *)realloc(c->seg, (size_t)c->cap_seg * sizeof(uint32_t));
+        if (!c->seg) { c->err = SG_ERR_NOMEM; return; }
+    }
+    for (m = k + 1; m < L->d; m++) lo += lv[m];
+    c->chains[c->nch].seg = (uint32_t)c->nseg;
+    c->chains[c->nch].sigma = (uint8_t)sigma;
+    c->chains[c->nch].lmax = (uint8_t)lmax;
+    c->chains[c->nch].lo = (uint8_t)lo;
+    c->chains[c->nch].pad = 0;
+    c->nch++;
+    for (j = 0; j <= lmax; j++) {
+        lv[k] = j;
+        c->seg[c->nseg++] = (uint32_t)sg_layout_subspace_offset(L, lv);
+    }
+    lv[k] = 0;
+}
+
+static int chain_size_cmp(const void *a, const void *b)
+{
+    const sg_chain *x = (const sg_chain *)a, *y = (const sg_chain *)b;
+    /* size = 2^sigma * (2^(lmax+1) - 1); compare exactly */
+    int64_t sx = ((int64_t)1 << x->sigma) * (((int64_t)2 << x->lmax) - 1);
+    int64_t sy = ((int64_t)1 << y->sigma) * (((int64_t)2 << y->lmax) - 1);
+    if (sx != sy) return sx > sy ? -1 : 1;
+    return x->seg < y->seg ? -1 : (x->seg > y->seg);
+}
+
+int sg_layout_chains(const sg_layout *L, int k, sg_chain **chains, int64_t *nchains,
+                     uint32_t **seg_off, int64_t *nseg)
+{
+    int dims[SG_MAX_DIMS], lv[SG_MAX_DIMS], m = 0, i;
+    chain_ctx c;
+    memset(&c, 0, sizeof(c));
+    memset(lv, 0, sizeof(lv));
+    c.L = L;
+    c.k = k;
+    for (i = 0; i < L->d; i++)
+        if (i != k) dims[m++] = i;
+    enum_levels(L, dims, m, 0, L->n - 1, 0, lv, chain_visit, &c);
+    if (c.err) {
+        free(c.chains);
+        free(c.seg);
+        return c.err;
+    }
+    if (c.nch > 1) qsort(c.chains, (size_t)c.nch, sizeof(sg_chain), chain_size_cmp);
+    *chains = c.chains;
+    *nchains = c.nch;
+    *seg_off = c.seg;
+    *nseg = c.nseg;
+    return SG_OK;
+}
+
+typedef struct {
+    const sg_layout *L;
+    uint32_t *off;
+    int64_t n;
+} dfs_ctx;
+
+static void dfs_visit(void *vctx, int *lv, int sum)
+{
+    dfs_ctx *c = (dfs_ctx *)vctx;
+    (void)sum;
+    c->off[c->n++] = (uint32_t)sg_layout_subspace_offset(c->L, lv);
+}
+
+int sg_layout_dfs_offsets(const sg_layout *L, uint32_t **off)
+{
+    int dims[SG_MAX_DIMS], lv[SG_MAX_DIMS], i;
+    dfs_ctx c;
+    for (i = 0; i < L->d; i++) dims[i] = i;
+    memset(lv, 0, sizeof(lv));
+    c.L = L;
+    c.n = 0;
+    c.off = (uint32_t *)malloc((size_t)(L->S > 0 ? L->S : 1) * sizeof(uint32_t));
+    if (!c.off) return SG_ERR_NOMEM;
+    enum_levels(L, dims, L->d, 0, L->n - 1, 0, lv, dfs_visit, &c);
+    if (c.n != L->S) {
+        free(c.off);
+        return SG_ERR_STATE;
+    }
+    *off = c.off;
+    return SG_OK;
+}

@@ -1,0 +1,348 @@
+#!/usr/bin/env python3
+"""Benchmark of the compact sparse-grid hot path on B200.
+
+Workload (the reference's at-scale GPU case): a regular sparse grid with
+d=10 and n=10 levels (N = 32,978,945 points, S = 92,378 subspaces, FP32),
+values f(x) = exp(-sum x_k^2) at the grid points; one step hierarchizes the
+grid from its nodal values and evaluates the interpolant at 2^24 query
+points uniform on [0,1)^10 (seed 1; rank r uses seed 1 + r).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One JSON line on rank 0.  `value` is whole-job evals/s with inputs resident
+in HBM; `e2e` is the same metric through the C ABI's host-buffer calls
+(sg_set_values / sg_hierarchize / sg_evaluate) with the host<->device copies
+inside the timed region.  Inputs (132 MB grid + 671 MB points per rank) are
+larger than the 126 MB L2, so no flush is needed between steps.
+`--impl reference` times the reference's own C/OpenMP code
+(omp_hierarchize3 + omp_evaluate5, compiled in place into oracle/_ref) on the
+host cores, on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+D, NLEV, M_EVAL, SEED = 10, 10, 1 << 24, 1
+WORKLOAD = "regular sparse grid d=10 n=10 (N=32,978,945), f=exp(-|x|^2), hierarchize + evaluate 2^24 uniform points"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--points", type=int, default=M_EVAL, help="query points per rank and step")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per reference sample")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.proc is None:
+            return
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        rows = getattr(self, "rows", [])
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def reference_cpu(values: np.ndarray, X: np.ndarray, seconds: float):
+    """Times the reference's own CPU path (oracle/_ref) on a bounded sample:
+    omp_hierarchize3 over the whole grid, omp_evaluate5 over as many query
+    points as fit in `seconds` (16K-point chunks: the SSE variant keeps the
+    coordinates in a stack array).  Returns (per-step evals/s, info)."""
+    from oracle.oracle import Reference
+    r = Reference(D, NLEV)
+    r.set_values(values)
+    t0 = time.perf_counter()
+    r.hierarchize(9)
+    t_h = time.perf_counter() - t0
+    probe = 2048
+    t0 = time.perf_counter()
+    r.evaluate(X[:probe], 7)
+    t_probe = time.perf_counter() - t0
+    m = int(min(X.shape[0], max(probe, probe * max(seconds - t_h, 1.0) / max(t_probe, 1e-6))))
+    m = max(probe, (m // 2048) * 2048)
+    t0 = time.perf_counter()
+    out = r.evaluate(X[:m], 7)
+    t_e = time.perf_counter() - t0
+    per_step = t_h + t_e * (M_EVAL / m)
+    info = {"cores": int(r.lib().ref_max_threads()), "t_hierarchize_s": t_h, "t_eval_sample_s": t_e,
+            "sample_points": m, "ref_out": out, "surplus": r.values()}
+    return M_EVAL / per_step, info
+
+
+def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsample: int = 192, ref_out=None):
+    """Max/relative error of the GPU results against the FP64 oracle on a
+    sample of query points (checker only)."""
+    from oracle.oracle import Oracle
+    o = Oracle(D, NLEV)
+    s64 = o.hierarchize_f64(values.astype(np.float64))
+    idx = np.linspace(0, X.shape[0] - 1, nsample).astype(np.int64)
+    u64 = o.evaluate_f64(s64, X[idx])
+    err = np.abs(gpu_out[idx].astype(np.float64) - u64)
+    scale = float(np.max(np.abs(u64)))
+    floor = 1e-3 * scale
+    res = {"points": int(nsample), "max_abs": float(err.max()), "norm_rel": float(err.max() / scale),
+           "max_rel_floor1e-3": float(np.max(err / np.maximum(np.abs(u64), floor)))}
+    if ref_out is not None:
+        e2 = np.abs(ref_out[idx[idx < ref_out.shape[0]]].astype(np.float64) - u64[idx < ref_out.shape[0]])
+        if e2.size:
+            res["reference_fp32_max_abs"] = float(e2.max())
+            res["reference_fp32_norm_rel"] = float(e2.max() / scale)
+    return res
+
+
+# ---------------------------------------------------------------------------
+def run_reference_arm(args, rank: int):
+    if rank != 0:
+        return
+    from adaptive_sparse_grid_bench_b200 import Grid, inputs
+    g = Grid(D, NLEV)
+    vals = inputs.grid_values(g, inputs.f_gauss)
+    X = inputs.uniform_points(SEED, min(args.points, 1 << 20), D)
+    vals_per = []
+    info = None
+    for it in range(args.warmup + args.steps):
+        v, info = reference_cpu(vals, X, args.cpu_seconds)
+        if it >= args.warmup:
+            vals_per.append(v)
+    value = float(statistics.mean(vals_per))
+    line = {
+        "impl": "reference", "metric": "evals/s", "value": value, "unit": "evals/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * M_EVAL / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded SplitMix64)",
+        "config": {"workload": WORKLOAD, "points_per_step": M_EVAL, "l2": "inputs larger than L2"},
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": info["cores"], "kind": "reference",
+                         "sample": (f"omp_hierarchize3 on the full grid + omp_evaluate5 on "
+                                    f"{info['sample_points']} of 2^24 points, extrapolated linearly")},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def device_inputs(g, rank, npts, torch, dev):
+    from adaptive_sparse_grid_bench_b200 import inputs
+    from adaptive_sparse_grid_bench_b200._lib import SG_FN_GAUSS
+    g.sample_function(SG_FN_GAUSS)
+    vals = torch.empty(g.num_points, dtype=torch.float32, device=dev)
+    g.get_values_device(vals)
+    torch.cuda.synchronize()
+    X = inputs.uniform_points(SEED + rank, npts, D)
+    return vals, X
+
+
+def run_b200(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+    from adaptive_sparse_grid_bench_b200 import Grid
+    from adaptive_sparse_grid_bench_b200._lib import SG_OPT_PROFILE
+
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    g = Grid(D, NLEV)
+    g.precision = args.precision
+    g.set_option(SG_OPT_PROFILE, 1)
+    vals_d, X = device_inputs(g, rank, args.points, torch, dev)
+    m = X.shape[0]
+    X_d = torch.from_numpy(X).to(dev)
+    out_d = torch.empty(m, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        g.set_values_device(vals_d, stream)
+        g.hierarchize_async(stream)
+        g.evaluate_device(X_d, out_d, m, stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    g.sync(stream)
+    barrier()
+    t_hier, t_eval, t_sort = [], [], []
+    with Clocks(local_rank) as clk:
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+            t = g.timings()  # waits for this step's phase events
+            t_hier.append(t["hierarchize"])
+            t_sort.append(t["sort"])
+            t_eval.append(t["evaluate"])
+        e1.record(stream)
+        barrier()
+    g.sync(stream)
+    ms = e0.elapsed_time(e1)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    value = world * m * args.steps / (ms_max / 1e3)
+
+    # end-to-end through the host-buffer C ABI, copies inside the timed region
+    e2e = None
+    if not args.no_e2e:
+        vals_h = torch.empty(g.num_points, dtype=torch.float32, pin_memory=True)
+        vals_h.copy_(vals_d)
+        X_h = torch.empty((m, D), dtype=torch.float32, pin_memory=True)
+        X_h.copy_(torch.from_numpy(X))
+        out_h = torch.empty(m, dtype=torch.float32, pin_memory=True)
+        vh, xh, oh = vals_h.numpy(), X_h.numpy(), out_h.numpy()
+        import ctypes
+        from adaptive_sparse_grid_bench_b200._lib import check, lib
+
+        def step_e2e():
+            check(lib().sg_set_values(g.handle, vh.ctypes.data))
+            check(lib().sg_hierarchize(g.handle))
+            check(lib().sg_evaluate(g.handle, xh.ctypes.data, oh.ctypes.data, ctypes.c_int64(m)))
+
+        step_e2e()
+        barrier()
+        s0 = torch.cuda.Event(enable_timing=True)
+        s1 = torch.cuda.Event(enable_timing=True)
+        s0.record()
+        for _ in range(args.steps):
+            step_e2e()
+        s1.record()
+        barrier()
+        e_ms = torch.tensor([s0.elapsed_time(s1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
+        e2e = {"value": world * m * args.steps / (float(e_ms.item()) / 1e3), "unit": "evals/s",
+               "h2d_bytes_per_step": int(g.num_points * 4 + m * D * 4), "d2h_bytes_per_step": int(m * 4)}
+        if not np.array_equal(oh, out_d.cpu().numpy()):
+            raise RuntimeError("host-buffer and device-pointer evaluations differ")
+
+    if rank != 0:
+        return
+    S = g.num_subspaces
+    hier_ms = statistics.mean(t_hier)
+    eval_ms = statistics.mean(t_eval)
+    hier_gbs = 8.0 * D * g.num_points / (hier_ms / 1e3) / 1e9
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        peak = float(json.load(open(peaks_path))["hbm_gbs"])
+        peak_src = "measured"
+    except (OSError, KeyError, ValueError):
+        peak, peak_src = 6650.0, "fallback"
+    eval_bytes = 4.0 * (S + D + 1) * m
+    achieved = eval_bytes / (eval_ms / 1e3) / 1e9
+    clocks = clk.summary()
+    line = {
+        "metric": "evals/s", "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64; values sampled on device)",
+        "config": {"workload": WORKLOAD, "points_per_step_per_rank": m, "d": D, "n": NLEV,
+                   "num_points": g.num_points, "num_subspaces": S, "hier_precision": args.precision,
+                   "l2": "inputs larger than L2 (132 MB grid + 671 MB points)", "parallelism": f"replicas x{world}"},
+        "hierarchize": {"value": hier_gbs, "unit": "GB/s", "ms": hier_ms, "bytes": "8*d*N"},
+        "evaluate": {"ms": eval_ms, "sort_ms": statistics.mean(t_sort), "evals_per_s": m / (eval_ms / 1e3),
+                     "pairs_per_s": m * S / (eval_ms / 1e3)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "kernel": "k_evaluate", "peak_source": peak_src,
+                     "bytes": "4*(S+d+1) per query point (cache-served surplus reads counted)"},
+        "e2e": e2e,
+        "gpu_launches": None,
+        "clocks": clocks,
+    }
+    # launches per step: set_values (n D2D copies are not kernels) + d sweeps
+    # (+2 conversions in fp64) + sort (memset is not a kernel: keys, 1-3 scan
+    # levels, scatter) + evaluate
+    sweeps = D + (2 if args.precision == "fp64" else 0)
+    line["gpu_launches"] = args.steps * (sweeps + 1 + 2 + 3 + 1)
+    if world == 1 and not args.no_cpu_baseline:
+        vals = vals_d.cpu().numpy()
+        cpu_v, info = reference_cpu(vals, X, args.cpu_seconds)
+        line["cpu_baseline"] = {"value": cpu_v, "unit": "evals/s", "cores": info["cores"], "kind": "reference",
+                                "sample": (f"reference omp_hierarchize3 on the full grid + omp_evaluate5 on "
+                                           f"{info['sample_points']} of 2^24 points, extrapolated linearly")}
+        line["err_vs_fp64"] = error_vs_fp64(vals, out_d.cpu().numpy(), X, ref_out=info["ref_out"])
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference_arm(args, rank)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,156 @@
+/*
+ * sgrid.h - C ABI of the B200 compact sparse-grid library (libsgb200.so).
+ *
+ * A drop-in for the callable surface of the reference benchmark
+ * adaptive_sparse_grid_bench.c (citations "c:LINE" refer to that file):
+ *
+ *   reference                                   this library
+ *   -----------------------------------------   ---------------------------
+ *   globals num_dims/num_levels/limits + init()  sg_create / sg_destroy
+ *     (c:77-85, c:101-140)
+ *   num_grid_points, num_subspaces (c:130-137)   sg_num_points/_subspaces
+ *   sg1d filled at the grid points (c:146-152)    sg_set_values
+ *   int hierarchizeK(void)  (c:557-1233)          sg_hierarchize
+ *   int evaluateK(sg1d, coord_mat, out, n)        sg_evaluate
+ *     (c:1237-1722)
+ *   int gp2idx(levels, indices)  (c:187-207)      sg_gp2idx
+ *   int idx2gp(index, levels, indices) (c:210)    sg_idx2gp
+ *   idx2l / l2idx  (c:245-279)                    sg_idx2l / sg_l2idx
+ *
+ * Conventions are the reference's: levels are 0-based, a grid of n levels
+ * holds every level vector l with sum(l) <= n-1 and l[k] <= limits[k]; point
+ * (l, i) sits at x = (2i+1)/2^(l+1); values, surpluses and the linear index
+ * follow the compact layout (level groups in order, subspaces by l2idx,
+ * points row-major with dim 0 most significant).  coord_mat is num_evals x d
+ * row-major floats in [0, 1).
+ *
+ * Every function returns an int status: SG_OK (0, the reference's
+ * "return 0") or a negative SG_ERR_* code; sg_last_error() gives the text.
+ * Host buffers belong to the caller; device memory belongs to the handle.
+ * A handle may be used by one host thread at a time.  sg_create touches no
+ * GPU: device storage is created on the current device by the first call
+ * that needs it.
+ */
+#ifndef SGRID_H
+#define SGRID_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SG_MAX_DIMS 20   /* the reference's CUDA cap (cu:17) */
+#define SG_MAX_LEVELS 16 /* n <= 16 (the reference's CUDA cap is 10, cu:18) */
+
+#define SG_OK 0
+#define SG_ERR_ARG (-1)     /* invalid argument                                */
+#define SG_ERR_RANGE (-2)   /* size beyond what the library supports           */
+#define SG_ERR_CUDA (-3)    /* a CUDA call failed                              */
+#define SG_ERR_NOMEM (-4)   /* host or device allocation failed                */
+#define SG_ERR_STATE (-5)   /* call out of order (e.g. no values set yet)      */
+#define SG_ERR_TIMEOUT (-6) /* a device-side wait gave up; results are invalid */
+
+/* Hierarchization precision (sg_set_option(SG_OPT_HIER_PRECISION, ...)). */
+#define SG_HIER_FP32 0 /* FP32 sweeps, bit-identical to hierarchize0 (c:557) */
+#define SG_HIER_FP64 1 /* FP64 sweeps, each surplus rounded once to FP32     */
+
+/* Options (sg_set_option / sg_get_option). */
+#define SG_OPT_HIER_PRECISION 1 /* SG_HIER_FP32 (default) or SG_HIER_FP64           */
+#define SG_OPT_EVAL_SORT 2      /* 1 (default): spatially order points on the GPU   */
+                                /* before evaluating; 0: evaluate in caller order    */
+#define SG_OPT_EVAL_PPT 3       /* points per thread in evaluate: 0 = auto, 1, 2     */
+#define SG_OPT_EVAL_BLOCKS 4    /* subspace blocking: number of passes, 0 = auto     */
+#define SG_OPT_HIER_KERNEL 5    /* 0 = auto, 1 = shared-memory chains, 2 = gather    */
+#define SG_OPT_PROFILE 6        /* 1: record CUDA events around each phase            */
+
+/* Phases reported by sg_timings (milliseconds of the most recent call). */
+#define SG_PHASE_HIERARCHIZE 0  /* all sweeps of the last hierarchization    */
+#define SG_PHASE_SORT 1         /* spatial ordering of the last evaluation  */
+#define SG_PHASE_EVALUATE 2     /* the evaluation kernel itself             */
+#define SG_NUM_PHASES 3
+
+typedef struct sg_grid sg_grid;
+
+/* ---- create / destroy (init(), c:101-140; cu:72-102) ------------------- */
+
+/* limits == NULL gives the regular grid (limits[k] = n-1, as c:1760-1763). */
+int sg_create(int d, int n, const int *limits, sg_grid **grid);
+int sg_destroy(sg_grid *grid);
+
+int sg_num_points(const sg_grid *grid, int64_t *num_points);       /* c:130-137 */
+int sg_num_subspaces(const sg_grid *grid, int64_t *num_subspaces); /* c:130-137 */
+int sg_dims(const sg_grid *grid, int *d, int *n, int *limits);
+
+/* dp[d*n]: dp[i*n+s] = number of level vectors over dims 0..i with sum s
+ * (dp_mat, c:113-129); lidx[n+1]: first index of each level group
+ * (lidx_vect, c:132-140, plus lidx[n] = num_points). */
+int sg_tables(const sg_grid *grid, int64_t *dp, int64_t *lidx);
+
+/* ---- index bijection (host; c:187-279) ---------------------------------- */
+int sg_gp2idx(const sg_grid *grid, const int *levels, const int *indices, int64_t *index);
+int sg_idx2gp(const sg_grid *grid, int64_t index, int *levels, int *indices);
+int sg_l2idx(const sg_grid *grid, const int *levels, int64_t *position);
+int sg_idx2l(const sg_grid *grid, int64_t position, int level_sum, int *levels);
+
+/* ---- host-buffer calls: synchronous, the reference's calling style ------ */
+
+/* values[num_points] in compact order (the sg1d fill of c:146-152). */
+int sg_set_values(sg_grid *grid, const float *values);
+/* Reads the grid back (surpluses after sg_hierarchize). */
+int sg_get_values(sg_grid *grid, float *values);
+/* In-place hierarchization of the stored values (hierarchize0..8, c:557). */
+int sg_hierarchize(sg_grid *grid);
+/* out[c] = interpolant at coord_mat[c*d .. c*d+d-1] (evaluate0..5, c:1237). */
+int sg_evaluate(sg_grid *grid, const float *coord_mat, float *out, int64_t num_evals);
+
+/* ---- device-pointer calls: asynchronous on `stream` (a cudaStream_t; NULL
+ *      is the legacy default stream).  Pointers are device memory. -------- */
+int sg_set_values_device(sg_grid *grid, const float *values, void *stream);
+int sg_get_values_device(sg_grid *grid, float *values, void *stream);
+int sg_hierarchize_async(sg_grid *grid, void *stream);
+int sg_evaluate_device(sg_grid *grid, const float *coord_mat, float *out,
+                       int64_t num_evals, void *stream);
+/* Waits for `stream` and reports any device-side error flag of the handle. */
+int sg_sync(sg_grid *grid, void *stream);
+
+/* Device bijection for batches (no reference counterpart beyond looping
+ * gp2idx/idx2gp; used to sample grids on the GPU).  levels/indices are
+ * count x d int32 row-major. */
+int sg_idx2gp_device(const sg_grid *grid, const int64_t *index, int *levels,
+                     int *indices, int64_t count, void *stream);
+int sg_gp2idx_device(const sg_grid *grid, const int *levels, const int *indices,
+                     int64_t *index, int64_t count, void *stream);
+
+/* Built-in test functions for sg_sample_function (evaluated in FP64 at the
+ * grid points, rounded once to FP32).  No reference counterpart beyond the
+ * sg1d fill of c:146-152, which samples SG_FN_REFERENCE on the host. */
+#define SG_FN_REFERENCE 0 /* sum_k x_k^2 (1 - x_k)^2  (fct, c:87-94)            */
+#define SG_FN_PROD4 1     /* prod_k 4 x_k (1 - x_k)                             */
+#define SG_FN_GAUSS 2     /* exp(-sum_k x_k^2)                                  */
+#define SG_FN_BUMP 3      /* exp(-p[1] sum_k (x_k - p[0])^2)                    */
+#define SG_FN_QUAD 4      /* prod_k (p[3k] + p[3k+1] x_k + p[3k+2] x_k^2)       */
+#define SG_MAX_FN_PARAMS 64
+
+/* Fills the grid with f at its points, on the device (replaces the value
+ * array like sg_set_values). */
+int sg_sample_function(sg_grid *grid, int fn, const double *params, int num_params, void *stream);
+
+/* ---- options and diagnostics ------------------------------------------ */
+int sg_set_option(sg_grid *grid, int option, int64_t value);
+int sg_get_option(const sg_grid *grid, int option, int64_t *value);
+/* Device time of each phase of the most recent calls made with
+ * SG_OPT_PROFILE on (waits for them); ms[SG_NUM_PHASES], -1 if not run. */
+int sg_timings(sg_grid *grid, double *ms);
+/* Bytes of device memory the handle holds (grid, tables and scratch). */
+int sg_device_bytes(const sg_grid *grid, int64_t *bytes);
+/* Text of the last error raised on the calling thread ("" if none). */
+const char *sg_last_error(void);
+/* Library version string. */
+const char *sg_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SGRID_H */

@@ -1,0 +1,202 @@
+"""GPU parity: the sm_100a kernels through the C ABI against the oracle and
+the reference's golden fixtures.
+
+Tolerances (stated here, used below):
+  - index bijection, grid structure: bit-exact;
+  - FP32 hierarchization: bit-exact with hierarchize0 (c:557-571);
+  - FP64 hierarchization: bit-exact with the FP64 oracle rounded once to FP32;
+  - evaluation: |gpu - oracle_fp64| <= EVAL_ATOL_REL * max|oracle_fp64| + EVAL_ATOL_ULP
+    (norm-wise relative error 1e-5 plus a few FP32 ulps of 1 for values near 0).
+"""
+import numpy as np
+import pytest
+
+import adaptive_sparse_grid_bench_b200 as sg
+from adaptive_sparse_grid_bench_b200 import inputs
+from conftest import golden_cases, load_golden
+from oracle.oracle import Oracle
+
+pytestmark = pytest.mark.gpu
+
+EVAL_RTOL_NORM = 1e-5
+EVAL_ATOL = 2e-7
+
+
+def _grid(d, n, lim=None, **opt):
+    g = sg.Grid(d, n, lim)
+    for k, v in opt.items():
+        g.set_option(k, v)
+    return g
+
+
+def assert_eval_close(got, ref64, what=""):
+    ref64 = np.asarray(ref64, np.float64)
+    scale = max(np.max(np.abs(ref64)), 1e-30)
+    err = np.abs(got.astype(np.float64) - ref64)
+    bound = EVAL_RTOL_NORM * scale + EVAL_ATOL
+    assert np.all(err <= bound), f"{what}: max err {err.max():.3e} > {bound:.3e} (max|u| {scale:.3e})"
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_hierarchize_bitexact(cuda, name):
+    gd = load_golden(name)
+    g = sg.Grid(int(gd["d"]), int(gd["n"]), gd["limits"])
+    assert g.num_points == int(gd["N"]) and g.num_subspaces == int(gd["S"])
+    g.set_values(gd["values"])
+    g.hierarchize()
+    h = g.get_values()
+    assert np.array_equal(h.view(np.uint32), gd["surplus"].view(np.uint32))
+
+
+@pytest.mark.parametrize("name", golden_cases())
+def test_golden_evaluate(cuda, name):
+    gd = load_golden(name)
+    d, n = int(gd["d"]), int(gd["n"])
+    g = sg.Grid(d, n, gd["limits"])
+    g.set_values(gd["surplus"])
+    o = Oracle(d, n, gd["limits"])
+    ref64 = o.evaluate_f64(gd["surplus"].astype(np.float64), gd["X"])
+    for sort in (0, 1):
+        g.set_option(sg.SG_OPT_EVAL_SORT, sort)
+        out = g.evaluate(gd["X"])
+        assert_eval_close(out, ref64, f"{name} sort={sort}")
+        # and against the reference's own FP32 evaluate0 at its own accuracy
+        np.testing.assert_allclose(out, gd["out"], rtol=0, atol=1e-5 * max(1.0, np.abs(gd["out"]).max()))
+    # the reference's correctness test: interpolation at grid points
+    outg = g.evaluate(gd["G"])
+    np.testing.assert_allclose(outg, gd["outG"], rtol=0, atol=1e-6)
+
+
+SHAPES = [
+    (1, 1, None), (1, 12, None), (2, 9, None), (3, 7, [6, 2, 4]), (4, 8, None), (5, 6, [5, 0, 5, 3, 1]),
+    (6, 6, None), (8, 5, None), (10, 5, None), (12, 4, None), (20, 3, None), (3, 12, None),
+]
+
+
+@pytest.mark.parametrize("d,n,lim", SHAPES)
+@pytest.mark.parametrize("kernel", [0, 2])
+def test_hierarchize_fp32_bitexact(cuda, d, n, lim, kernel):
+    o = Oracle(d, n, lim)
+    g = _grid(d, n, lim, **{sg.SG_OPT_HIER_KERNEL: kernel})
+    v = inputs.uniform01(d * 31 + n, g.num_points) * 2 - 1
+    g.set_values(v)
+    g.hierarchize()
+    got = g.get_values()
+    want = o.hierarchize_f32(v)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("d,n,lim", SHAPES)
+@pytest.mark.parametrize("kernel", [0, 2])
+def test_hierarchize_fp64_matches_fp64_oracle(cuda, d, n, lim, kernel):
+    o = Oracle(d, n, lim)
+    g = _grid(d, n, lim, **{sg.SG_OPT_HIER_KERNEL: kernel, sg.SG_OPT_HIER_PRECISION: sg.SG_HIER_FP64})
+    v = inputs.uniform01(d * 17 + n, g.num_points) * 2 - 1
+    g.set_values(v)
+    g.hierarchize()
+    got = g.get_values()
+    want = o.hierarchize_f64(v.astype(np.float64)).astype(np.float32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("d,n,lim", [(4, 8, None), (3, 7, [6, 2, 4]), (10, 5, None), (1, 12, None), (6, 6, None)])
+@pytest.mark.parametrize("ppt", [1, 2])
+def test_evaluate_vs_fp64_oracle(cuda, d, n, lim, ppt):
+    o = Oracle(d, n, lim)
+    g = _grid(d, n, lim, **{sg.SG_OPT_EVAL_PPT: ppt})
+    vals = inputs.grid_values(g, inputs.f_gauss)
+    g.set_values(vals)
+    g.hierarchize()
+    surplus = g.get_values()
+    X = inputs.uniform_points(5, 777, d)
+    ref64 = o.evaluate_f64(surplus.astype(np.float64), X)
+    for sort in (1, 0):
+        g.set_option(sg.SG_OPT_EVAL_SORT, sort)
+        assert_eval_close(g.evaluate(X), ref64, f"d={d} n={n} sort={sort} ppt={ppt}")
+
+
+def test_evaluate_edge_coordinates(cuda):
+    d, n = 3, 6
+    o = Oracle(d, n)
+    g = sg.Grid(d, n)
+    g.set_values(inputs.grid_values(g, inputs.f_prod4))
+    g.hierarchize()
+    s = g.get_values()
+    below1 = np.nextafter(np.float32(1), np.float32(0))
+    X = np.array([[0, 0, 0], [below1] * 3, [0.5, 0.5, 0.5], [0, 0.5, below1],
+                  [2.0 ** -24, 0.25, 0.75]], np.float32)
+    assert_eval_close(g.evaluate(X), o.evaluate_f64(s.astype(np.float64), X), "edges")
+    # outside [0,1)^d every basis function vanishes: 0 (NaN stays NaN)
+    Y = np.array([[1.0, 0.5, 0.5], [-0.1, 0.5, 0.5], [0.5, 3.0, 0.5], [np.nan, 0.5, 0.5]], np.float32)
+    out = g.evaluate(Y)
+    assert np.array_equal(out[:3], np.zeros(3, np.float32)) and np.isnan(out[3])
+
+
+@pytest.mark.parametrize("m", [0, 1, 2, 31, 33, 255, 257, 4099])
+def test_evaluate_ragged_counts(cuda, m):
+    d, n = 5, 5
+    o = Oracle(d, n)
+    g = sg.Grid(d, n)
+    g.set_values(inputs.grid_values(g, inputs.f_gauss))
+    g.hierarchize()
+    s = g.get_values()
+    X = inputs.uniform_points(m + 3, m, d)
+    out = g.evaluate(X)
+    assert out.shape == (m,)
+    if m:
+        assert_eval_close(out, o.evaluate_f64(s.astype(np.float64), X), f"m={m}")
+
+
+def test_evaluate_device_api_and_repeat(cuda):
+    import torch
+    d, n = 4, 8
+    g = sg.Grid(d, n)
+    vals = inputs.grid_values(g, inputs.f_prod4)
+    dv = torch.from_numpy(vals).to(cuda)
+    g.set_values_device(dv)
+    g.hierarchize_async()
+    X = inputs.uniform_points(0, 65536, d)
+    dX = torch.from_numpy(X).to(cuda)
+    out1 = torch.empty(X.shape[0], device=cuda)
+    out2 = torch.empty(X.shape[0], device=cuda)
+    g.evaluate_device(dX, out1)
+    g.evaluate_device(dX, out2)
+    g.sync()
+    assert torch.equal(out1, out2)
+    host = g.evaluate(X)
+    assert np.array_equal(host, out1.cpu().numpy())
+    back = torch.empty(g.num_points, device=cuda)
+    g.get_values_device(back)
+    g.sync()
+    assert np.array_equal(back.cpu().numpy(), g.get_values())
+
+
+def test_device_bijection(cuda):
+    import torch
+    for d, n, lim in [(4, 8, None), (3, 7, [6, 2, 4]), (10, 5, None)]:
+        g = sg.Grid(d, n, lim)
+        o = Oracle(d, n, lim)
+        idx = torch.arange(g.num_points, dtype=torch.int64, device=cuda)
+        lv = torch.empty((g.num_points, d), dtype=torch.int32, device=cuda)
+        ix = torch.empty_like(lv)
+        g.idx2gp_device(idx, lv, ix, g.num_points)
+        back = torch.empty_like(idx)
+        g.gp2idx_device(lv, ix, back, g.num_points)
+        torch.cuda.synchronize()
+        assert torch.equal(back, idx)
+        lvh, ixh = lv.cpu().numpy(), ix.cpu().numpy()
+        for i in range(0, g.num_points, max(1, g.num_points // 300)):
+            a, b = o.idx2gp(i)
+            assert np.array_equal(lvh[i], a) and np.array_equal(ixh[i], b)
+
+
+def test_errors_on_gpu(cuda):
+    g = sg.Grid(3, 4)
+    with pytest.raises(sg.SgError) as e:
+        g.hierarchize()
+    assert e.value.code == -5  # no values yet
+    with pytest.raises(sg.SgError):
+        g.evaluate(np.zeros((4, 3), np.float32))
+    g.set_values(np.ones(g.num_points, np.float32))
+    with pytest.raises(ValueError):
+        g.set_values(np.ones(g.num_points + 1, np.float32))
