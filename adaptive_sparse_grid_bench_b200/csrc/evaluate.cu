@@ -8,20 +8,23 @@
  * the subspace (dim 0 most significant) and hat_k = 1 - |x_k 2^(l_k+1) - (2t_k+1)|.
  *
  * B200 design.  One thread owns PPT query points; every warp walks the same
- * depth-first tree over level vectors (dims 0..d-1, each dim's level
- * ascending, sum(l) <= n-1, l_k <= limits[k]), so the loop structure is
+ * depth-first tree over the level vectors of the prefix dims 0..d-3 (each
+ * dim's level ascending, sum(l) <= n-1, l_k <= limits[k]), so control flow is
  * uniform across the warp and partial products / partial cell indices are
- * shared between all subspaces of a subtree:
- *   - at depth k the next level's fractional part, cell index and hat come
- *     from the previous level's with a doubling (exact in FP32), so no
- *     division, no float->int conversion and no table appears in the walk;
- *   - the innermost dim's hats and cell indices are precomputed once per
- *     point in registers; its loop (one subspace per iteration) is one
- *     shift-add, one gather and one FMA per point;
- *   - subspace offsets come from a depth-first offset table (one broadcast
- *     load per subspace, shared by the whole warp);
- *   - the innermost partial sum is folded into a Kahan-compensated
- *     accumulator (compensated summation over subspaces).
+ * shared by all subspaces below a node.  At depth d-2 the walk reaches a
+ * block: every subspace of the two innermost dims (A = d-2, B = d-1) under
+ * that prefix, stored contiguously per prefix cell in the block layout (see
+ * sg_layout.h), with dim B's levels as a 1-D heap.  The surplus of (a, b) is
+ * then at base + aoff(a) + t_a*plen(a) + (2^b - 1 + t_b):
+ *   - base is one multiply-add per block and point; the row offset one
+ *     multiply-add per row; 2^b - 1 + t_b and the hats of dims A and B are
+ *     precomputed per point in registers, so each subspace costs one add,
+ *     one gather and one FMA;
+ *   - blocks of budget R < 12 (all of them in regular grids up to n = 12)
+ *     run fully unrolled, so a block's gathers issue back to back;
+ *   - hats of the prefix dims come from the previous level's with a doubling
+ *     (exact in FP32), so no division or table appears in the walk;
+ *   - each block's partial sum enters a Kahan-compensated accumulator.
  * Query points are first put in spatial (Morton) order on the GPU so that
  * the 32 points of a warp land in few cells of each subspace: the gathers
  * then touch few sectors and the grid is served from L1/L2.
@@ -34,17 +37,20 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kNL = SG_MAX_LEVELS; /* register arrays sized for any n */
+constexpr int kNB = 12; /* blocks with level budget R < kNB run fully unrolled */
+constexpr int kTB = 15; /* T = floor(x 2^15) holds the cells of levels 0..15  */
 
 struct EvalArgs {
-    const float *__restrict__ alpha;
-    const uint32_t *__restrict__ leaf;
+    const float *__restrict__ alpha;          /* block layout                 */
+    const uint32_t *__restrict__ prefix_base; /* one block base per prefix    */
     const float *__restrict__ coords;
     const int32_t *__restrict__ perm;
     float *__restrict__ out;
     int64_t num_evals;
-    int nm1;
+    int nm1;                                  /* n - 1                        */
+    int regular2;                             /* last two dims unrestricted   */
     int lim[SG_MAX_DIMS];
+    uint32_t blk[SG_MAX_LEVELS];              /* block size per budget R      */
 };
 
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
@@ -61,31 +67,141 @@ __device__ __forceinline__ float hat_of(float y)
     return 1.0f - fabsf(fmaf(2.0f, y, -1.0f));
 }
 
+/* next level: y <- frac(2y), t <- 2t + floor(2y); exact in FP32 */
+__device__ __forceinline__ void step_level(float &y, uint32_t &t)
+{
+    const float y2 = y + y;
+    const bool b = y2 >= 1.0f;
+    y = b ? y2 - 1.0f : y2;
+    t = (t << 1) | (uint32_t)b;
+}
+
+/* Per-point values of the two innermost dims (A = d-2, B = d-1). */
+template <int P>
+struct Inner {
+    float hB[P][kNB];    /* hat of dim B at level b                      */
+    uint32_t cB[P][kNB]; /* heap index 2^b - 1 + t_b of dim B            */
+    float hA[P][kNB];    /* hat of dim A at level a                      */
+    uint32_t TA[P];      /* floor(x_A 2^15): t_a = TA >> (15 - a)        */
+};
+
+__host__ __device__ constexpr uint32_t aoff_reg(int R, int a)
+{
+    uint32_t o = 0;
+    for (int q = 0; q < a; ++q) o += (1u << q) * ((2u << (R - q)) - 1u);
+    return o;
+}
+
+/* One block of budget R of a grid whose last two dims are unrestricted:
+ * rows a = 0..R, row a holds 2^a poles of R-a+1 levels.  Fully unrolled:
+ * one add, one gather and one FMA per subspace and point. */
+template <int R, int P>
+__device__ __forceinline__ void block_fixed(const float *__restrict__ alpha, const uint32_t (&base)[P],
+                                            const Inner<P> &in, float (&s)[P])
+{
+#pragma unroll
+    for (int a = 0; a <= R; ++a) {
+        const uint32_t plen = (2u << (R - a)) - 1u;
+        const uint32_t ao = aoff_reg(R, a);
+        uint32_t rb[P];
+        float sr[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            rb[p] = base[p] + ao + (in.TA[p] >> (kTB - a)) * plen;
+            sr[p] = 0.0f;
+        }
+#pragma unroll
+        for (int b = 0; b <= R - a; ++b)
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                sr[p] = fmaf(in.hB[p][b], __ldg(alpha + rb[p] + in.cB[p][b]), sr[p]);
+#pragma unroll
+        for (int p = 0; p < P; ++p) s[p] = fmaf(in.hA[p][a], sr[p], s[p]);
+    }
+}
+
+template <int R, int P>
+__device__ __forceinline__ bool block_dispatch(int r, const float *__restrict__ alpha, const uint32_t (&base)[P],
+                                               const Inner<P> &in, float (&s)[P])
+{
+    if (r == R) {
+        block_fixed<R, P>(alpha, base, in, s);
+        return true;
+    }
+    if constexpr (R + 1 < kNB) return block_dispatch<R + 1, P>(r, alpha, base, in, s);
+    return false;
+}
+
+/* Any block: runtime loops, hats stepped level by level (limits on the last
+ * two dims, budgets R >= kNB, and d = 1 where dim A is absent). */
+template <int D, int P>
+__device__ __forceinline__ void block_generic(const EvalArgs &A, int R, const float (&x)[P][D],
+                                              const uint32_t (&base)[P], float (&s)[P])
+{
+    const int limA = D >= 2 ? A.lim[D - 2] : 0;
+    const int limB = A.lim[D - 1];
+    const int amax = min(R, limA);
+    uint32_t aoff = 0;
+    float yA[P];
+    uint32_t tA[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        yA[p] = D >= 2 ? x[p][D >= 2 ? D - 2 : 0] : 0.0f;
+        tA[p] = 0;
+    }
+    for (int a = 0; a <= amax; ++a) {
+        if (a) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) step_level(yA[p], tA[p]);
+        }
+        const int rl = min(R - a, limB) + 1;
+        const uint32_t plen = (1u << rl) - 1u;
+        float yB[P], sr[P];
+        uint32_t tB[P], rb[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            yB[p] = x[p][D - 1];
+            tB[p] = 0;
+            sr[p] = 0.0f;
+            rb[p] = base[p] + aoff + tA[p] * plen;
+        }
+        for (int b = 0; b < rl; ++b) {
+            if (b) {
+#pragma unroll
+                for (int p = 0; p < P; ++p) step_level(yB[p], tB[p]);
+            }
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                sr[p] = fmaf(hat_of(yB[p]), __ldg(A.alpha + rb[p] + (1u << b) - 1u + tB[p]), sr[p]);
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) s[p] = fmaf(D >= 2 ? hat_of(yA[p]) : 1.0f, sr[p], s[p]);
+        aoff += (1u << a) * plen;
+    }
+}
+
+/* Depth-first walk over the prefix dims 0..D-3; at depth D-2 one block. */
 template <int D, int K, int P>
 struct Walk {
-    static __device__ __forceinline__ void run(const EvalArgs &A, int budget, int &leaf,
-                                               const float (&x)[P][D], const uint32_t (&T)[P],
-                                               const float (&hl)[P][kNL], const float (&pin)[P],
-                                               const uint32_t (&iin)[P], float (&sum)[P],
-                                               float (&comp)[P])
+    static __device__ __forceinline__ void run(const EvalArgs &A, int budget, int &pc, const float (&x)[P][D],
+                                               const Inner<P> &in, const float (&pin)[P],
+                                               const uint32_t (&iin)[P], float (&sum)[P], float (&comp)[P])
     {
-        if constexpr (K == D - 1) {
-            /* innermost dim: one subspace per level j */
-            const int jmax = min(A.lim[K], budget);
+        if constexpr (K >= D - 2) {
+            const int R = budget;
+            const uint32_t bb = __ldg(A.prefix_base + pc);
+            ++pc;
+            const uint32_t blk = A.blk[R];
+            uint32_t base[P];
             float s[P];
 #pragma unroll
-            for (int p = 0; p < P; ++p) s[p] = 0.0f;
-#pragma unroll
-            for (int j = 0; j < kNL; ++j) {
-                if (j > jmax) break;
-                const uint32_t off = __ldg(A.leaf + leaf + j);
-#pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    const uint32_t idx = (iin[p] << j) + (T[p] >> (kNL - 1 - j));
-                    s[p] = fmaf(hl[p][j], __ldg(A.alpha + off + idx), s[p]);
-                }
+            for (int p = 0; p < P; ++p) {
+                base[p] = bb + iin[p] * blk;
+                s[p] = 0.0f;
             }
-            leaf += jmax + 1;
+            bool done = false;
+            if (D >= 2 && A.regular2) done = block_dispatch<0, P>(R, A.alpha, base, in, s);
+            if (!done) block_generic<D, P>(A, R, x, base, s);
 #pragma unroll
             for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], pin[p] * s[p]);
         } else {
@@ -102,21 +218,18 @@ struct Walk {
                 if (l) {
 #pragma unroll
                     for (int p = 0; p < P; ++p) {
-                        const float y2 = y[p] + y[p];
-                        const bool b = y2 >= 1.0f;
-                        y[p] = b ? y2 - 1.0f : y2;
-                        t[p] = (t[p] << 1) | (uint32_t)b;
+                        step_level(y[p], t[p]);
                         J[p] <<= 1;
                     }
                 }
                 float pn[P];
-                uint32_t in[P];
+                uint32_t ix[P];
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
                     pn[p] = pin[p] * hat_of(y[p]);
-                    in[p] = J[p] + t[p];
+                    ix[p] = J[p] + t[p];
                 }
-                Walk<D, K + 1, P>::run(A, budget - l, leaf, x, T, hl, pn, in, sum, comp);
+                Walk<D, K + 1, P>::run(A, budget - l, pc, x, in, pn, ix, sum, comp);
             }
         }
     }
@@ -153,18 +266,24 @@ __global__ void __launch_bounds__(kThreads) k_evaluate(const EvalArgs A)
         valid[p] = valid[p] && inside;
     }
 
-    /* innermost dim: hats and cell indices of every level */
-    uint32_t T[P];
-    float hl[P][kNL];
+    Inner<P> in;
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         float y = x[p][D - 1];
-        T[p] = (uint32_t)(y * (float)(1u << (kNL - 1)));
+        uint32_t t = 0;
 #pragma unroll
-        for (int j = 0; j < kNL; ++j) {
-            hl[p][j] = hat_of(y);
-            const float y2 = y + y;
-            y = y2 >= 1.0f ? y2 - 1.0f : y2;
+        for (int j = 0; j < kNB; ++j) {
+            if (j) step_level(y, t);
+            in.hB[p][j] = hat_of(y);
+            in.cB[p][j] = ((1u << j) - 1u) + t;
+        }
+        const float xa = D >= 2 ? x[p][D >= 2 ? D - 2 : 0] : 0.0f;
+        in.TA[p] = (uint32_t)(xa * (float)(1u << kTB));
+        y = xa;
+#pragma unroll
+        for (int j = 0; j < kNB; ++j) {
+            if (j) y = (y + y >= 1.0f) ? y + y - 1.0f : y + y;
+            in.hA[p][j] = hat_of(y);
         }
     }
 
@@ -177,8 +296,8 @@ __global__ void __launch_bounds__(kThreads) k_evaluate(const EvalArgs A)
         sum[p] = 0.0f;
         comp[p] = 0.0f;
     }
-    int leaf = 0;
-    Walk<D, 0, P>::run(A, A.nm1, leaf, x, T, hl, pin, iin, sum, comp);
+    int pc = 0;
+    Walk<D, 0, P>::run(A, A.nm1, pc, x, in, pin, iin, sum, comp);
 
 #pragma unroll
     for (int p = 0; p < P; ++p) {
@@ -205,6 +324,23 @@ int dispatch_ppt(const EvalArgs &A, int ppt, void *stream)
 {
     if (ppt == 2) return launch_eval<D, 2>(A, stream);
     return launch_eval<D, 1>(A, stream);
+}
+
+/* compact (group-aligned) layout -> block layout, one CTA per subspace */
+__global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
+                         const sg_repack *__restrict__ rp, int64_t nsub)
+{
+    for (int64_t q = blockIdx.x; q < nsub; q += gridDim.x) {
+        const sg_repack r = rp[q];
+        const int n = 1 << r.s;
+        const int ab = r.a + r.b;
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            const uint32_t I = (uint32_t)e >> ab;
+            const uint32_t ta = ((uint32_t)e >> r.b) & ((1u << r.a) - 1u);
+            const uint32_t tb = (uint32_t)e & ((1u << r.b) - 1u);
+            dst[r.dst + I * r.blk + ta * r.plen + tb] = src[r.src + e];
+        }
+    }
 }
 
 /* ---- spatial ordering of the query points ------------------------------ */
@@ -340,13 +476,15 @@ int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm
     if (num_evals <= 0) return cudaSuccess;
     EvalArgs A;
     A.alpha = p->alpha;
-    A.leaf = p->leaf;
+    A.prefix_base = p->prefix_base;
     A.coords = coords;
     A.perm = perm;
     A.out = out;
     A.num_evals = num_evals;
     A.nm1 = p->n - 1;
     for (int k = 0; k < SG_MAX_DIMS; ++k) A.lim[k] = k < p->d ? p->lim[k] : 0;
+    for (int r = 0; r < SG_MAX_LEVELS; ++r) A.blk[r] = p->blk[r];
+    A.regular2 = p->d >= 2 && p->lim[p->d - 2] >= p->n - 1 && p->lim[p->d - 1] >= p->n - 1;
     const int ppt = p->ppt;
     switch (p->d) {
 #define SG_D(DD) \
@@ -357,6 +495,14 @@ int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm
 #undef SG_D
     default: return cudaErrorInvalidValue;
     }
+}
+
+int sgk_repack(const float *src, float *dst, const sg_repack *rp, int64_t nsub, void *stream)
+{
+    if (nsub <= 0) return cudaSuccess;
+    int64_t g = nsub < 148 * 64 ? nsub : 148 * 64;
+    k_repack<<<(unsigned)g, 128, 0, (cudaStream_t)stream>>>(src, dst, rp, nsub);
+    return cudaGetLastError();
 }
 
 int64_t sgk_sort_scratch_bytes(int64_t num_evals, int d)

@@ -40,12 +40,17 @@ int sgk_narrow(const double *src, float *dst, int64_t n, void *stream);
 
 /* Evaluation. */
 typedef struct sg_eval_plan {
-    const float *alpha;     /* device grid, group-aligned layout             */
-    const uint32_t *leaf;   /* device: subspace offsets in depth-first order */
+    const float *alpha;          /* device grid in the block layout          */
+    const uint32_t *prefix_base; /* device: block base of every prefix       */
     int d, n;
     int lim[SG_MAX_DIMS];
-    int ppt;                /* points per thread (1 or 2)                    */
+    uint32_t blk[SG_MAX_LEVELS]; /* block size for each level budget R       */
+    int ppt;                     /* points per thread (1 or 2)               */
 } sg_eval_plan;
+
+/* Reorders the surpluses from the group-aligned compact layout into the
+ * block layout (one descriptor per subspace). */
+int sgk_repack(const float *src, float *dst, const sg_repack *rp, int64_t nsub, void *stream);
 
 /* out[perm ? perm[i] : i] = interpolant at coords[i*d .. i*d+d-1]. */
 int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm,

@@ -210,34 +210,120 @@ int sg_layout_chains(const sg_layout *L, int k, sg_chain **chains, int64_t *ncha
     return SG_OK;
 }
 
-typedef struct {
-    const sg_layout *L;
-    uint32_t *off;
-    int64_t n;
-} dfs_ctx;
+/* ---- evaluation (block) layout ------------------------------------------ */
 
-static void dfs_visit(void *vctx, int *lv, int sum)
+void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh)
 {
-    dfs_ctx *c = (dfs_ctx *)vctx;
-    (void)sum;
-    c->off[c->n++] = (uint32_t)sg_layout_subspace_offset(c->L, lv);
+    const int d = L->d;
+    const int limA = d >= 2 ? L->lim[d - 2] : 0;
+    const int limB = L->lim[d - 1];
+    int a;
+    uint32_t off = 0;
+    memset(sh, 0, sizeof(*sh));
+    sh->R = R;
+    sh->amax = R < limA ? R : limA;
+    for (a = 0; a <= sh->amax; a++) {
+        int rl = R - a < limB ? R - a : limB;
+        sh->rowlen[a] = rl + 1;
+        sh->aoff[a] = off;
+        off += ((uint32_t)1 << a) * (((uint32_t)1 << (rl + 1)) - 1);
+    }
+    sh->aoff[sh->amax + 1] = off;
 }
 
-int sg_layout_dfs_offsets(const sg_layout *L, uint32_t **off)
+typedef struct {
+    const sg_layout *L;
+    uint32_t *base;
+    int64_t np, cap;
+    uint32_t next;
+    int err;
+} prefix_ctx;
+
+static void prefix_visit(void *vctx, int *lv, int sigma)
 {
-    int dims[SG_MAX_DIMS], lv[SG_MAX_DIMS], i;
-    dfs_ctx c;
-    for (i = 0; i < L->d; i++) dims[i] = i;
+    prefix_ctx *c = (prefix_ctx *)vctx;
+    sg_eval_shape sh;
+    (void)lv;
+    if (c->err) return;
+    if (c->np == c->cap) {
+        c->cap = c->cap ? 2 * c->cap : 1024;
+        c->base = (uint32_t *)realloc(c->base, (size_t)c->cap * sizeof(uint32_t));
+        if (!c->base) { c->err = SG_ERR_NOMEM; return; }
+    }
+    sg_layout_eval_shape(c->L, c->L->n - 1 - sigma, &sh);
+    c->base[c->np++] = c->next;
+    c->next += ((uint32_t)1 << sigma) * sh.aoff[sh.amax + 1];
+}
+
+int sg_layout_eval_tables(const sg_layout *L, uint32_t **prefix_base, int64_t *nprefix,
+                          sg_repack **repack)
+{
+    const int d = L->d;
+    const int np_dims = d >= 2 ? d - 2 : 0; /* dims 0..d-3 form the prefix */
+    int dims[SG_MAX_DIMS], lv[SG_MAX_DIMS], i, s, k, R;
+    int64_t pos, r = 0;
+    int64_t cnt[SG_MAX_DIMS + 1][SG_MAX_LEVELS]; /* completions of dims k.. with sum <= R */
+    prefix_ctx c;
+    sg_repack *rp;
+    for (R = 0; R < L->n; R++) cnt[np_dims][R] = 1;
+    for (k = np_dims - 1; k >= 0; k--)
+        for (R = 0; R < L->n; R++) {
+            int l;
+            int64_t v = 0;
+            for (l = 0; l <= R && l <= L->lim[k]; l++) v += cnt[k + 1][R - l];
+            cnt[k][R] = v;
+        }
+    memset(&c, 0, sizeof(c));
     memset(lv, 0, sizeof(lv));
     c.L = L;
-    c.n = 0;
-    c.off = (uint32_t *)malloc((size_t)(L->S > 0 ? L->S : 1) * sizeof(uint32_t));
-    if (!c.off) return SG_ERR_NOMEM;
-    enum_levels(L, dims, L->d, 0, L->n - 1, 0, lv, dfs_visit, &c);
-    if (c.n != L->S) {
-        free(c.off);
+    for (i = 0; i < np_dims; i++) dims[i] = i;
+    enum_levels(L, dims, np_dims, 0, L->n - 1, 0, lv, prefix_visit, &c);
+    if (c.err) {
+        free(c.base);
+        return c.err;
+    }
+    if ((int64_t)c.next != L->N) {
+        free(c.base);
         return SG_ERR_STATE;
     }
-    *off = c.off;
+    rp = (sg_repack *)malloc((size_t)(L->S > 0 ? L->S : 1) * sizeof(sg_repack));
+    if (!rp) {
+        free(c.base);
+        return SG_ERR_NOMEM;
+    }
+    /* prefix index of a level vector: rank of its first d-2 levels in the
+     * depth-first enumeration; found by a second walk keyed on the vector */
+    for (s = 0; s < L->n; s++)
+        for (pos = 0; pos < L->dp[d - 1][s]; pos++) {
+            int a, b, sigma = 0;
+            int64_t pidx = 0;
+            sg_eval_shape sh;
+            sg_layout_idx2l(L, pos, s, lv);
+            /* rank among prefixes: count prefixes that precede lv[0..d-3] */
+            {
+                int rem = L->n - 1;
+                for (k = 0; k < np_dims; k++) {
+                    int l;
+                    for (l = 0; l < lv[k]; l++) pidx += cnt[k + 1][rem - l];
+                    rem -= lv[k];
+                }
+            }
+            for (k = 0; k < np_dims; k++) sigma += lv[k];
+            a = d >= 2 ? lv[d - 2] : 0;
+            b = lv[d - 1];
+            sg_layout_eval_shape(L, L->n - 1 - sigma, &sh);
+            rp[r].src = (uint32_t)(L->plidx[s] + (pos << s));
+            rp[r].dst = c.base[pidx] + sh.aoff[a] + (((uint32_t)1 << b) - 1);
+            rp[r].blk = sh.aoff[sh.amax + 1];
+            rp[r].plen = ((uint32_t)1 << sh.rowlen[a]) - 1;
+            rp[r].a = (uint8_t)a;
+            rp[r].b = (uint8_t)b;
+            rp[r].s = (uint8_t)s;
+            rp[r].pad = 0;
+            r++;
+        }
+    *prefix_base = c.base;
+    *nprefix = c.np;
+    *repack = rp;
     return SG_OK;
 }

@@ -56,10 +56,40 @@ int64_t sg_layout_subspace_offset(const sg_layout *L, const int *lv);
 int sg_layout_chains(const sg_layout *L, int k, sg_chain **chains, int64_t *nchains,
                      uint32_t **seg_off, int64_t *nseg);
 
-/* Device offsets of all subspaces in evaluation (depth-first) order: dims
- * 0..d-1 outermost to innermost, each dim's level ascending.  *off is
- * malloc'd with S entries. */
-int sg_layout_dfs_offsets(const sg_layout *L, uint32_t **off);
+
+/*
+ * Evaluation layout ("block layout").  The same surpluses, ordered for the
+ * evaluation walk: for every prefix level vector p of dims 0..d-3 (depth-
+ * first order, level ascending), for every cell I of p (row-major over those
+ * dims), one block holding all subspaces (p, a, b) with a = l_{d-2},
+ * b = l_{d-1}: rows a = 0..amax, each row 2^a poles (one per cell t_a of dim
+ * d-2), each pole the 1-D heap of dim d-1's levels b = 0..rowlen(a)-1 with
+ * cell t_b of level b at heap index 2^b - 1 + t_b.  A query point therefore
+ * finds every surplus of a block at base + aoff(a) + t_a*plen(a) + 2^b-1 + t_b.
+ * For d = 1 the "block" is the single pole of dim 0 (one row, a = 0).
+ */
+typedef struct sg_eval_shape {
+    int R;         /* level budget n-1-sigma left for the last two dims */
+    int amax;      /* last row: min(R, lim_{d-2}) (0 for d = 1)          */
+    int rowlen[SG_MAX_LEVELS]; /* levels of dim d-1 in row a             */
+    uint32_t aoff[SG_MAX_LEVELS + 1]; /* row starts; aoff[amax+1] = block size */
+} sg_eval_shape;
+
+void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh);
+
+/* Per-subspace repack descriptor (compact layout -> block layout). */
+typedef struct sg_repack {
+    uint32_t src;  /* device offset of the subspace in the group-aligned layout */
+    uint32_t dst;  /* block-layout offset of its element (I=0, t_a=0, t_b=0)    */
+    uint32_t blk;  /* block size: stride between prefix cells I                */
+    uint32_t plen; /* pole length of its row: stride between cells t_a         */
+    uint8_t a, b, s, pad;
+} sg_repack;
+
+/* Block bases (one per prefix, depth-first order) and the repack table (one
+ * entry per subspace).  Both malloc'd. */
+int sg_layout_eval_tables(const sg_layout *L, uint32_t **prefix_base, int64_t *nprefix,
+                          sg_repack **repack);
 
 #ifdef __cplusplus
 }

@@ -26,7 +26,11 @@ struct sg_grid {
     int64_t opt[NOPT];
     float *d_alpha;   /* Npad floats, group-aligned layout         */
     double *d_work;   /* Npad doubles, FP64 hierarchization (lazy) */
-    uint32_t *d_leaf; /* S subspace offsets, depth-first order     */
+    float *d_blk;        /* N floats: surpluses in the block layout    */
+    uint32_t *d_prefix;  /* block base per prefix                      */
+    sg_repack *d_repack; /* per-subspace compact -> block descriptors  */
+    uint32_t blk[SG_MAX_LEVELS]; /* block size per level budget         */
+    int eval_dirty;      /* d_blk is stale                              */
     sg_chain *d_chains[SG_MAX_DIMS];
     uint32_t *d_seg[SG_MAX_DIMS];
     sg_sweep_tables sweep[SG_MAX_DIMS];
@@ -104,7 +108,9 @@ static void free_device(sg_grid *g)
         }
     cudaFree(g->d_alpha);
     cudaFree(g->d_work);
-    cudaFree(g->d_leaf);
+    cudaFree(g->d_blk);
+    cudaFree(g->d_prefix);
+    cudaFree(g->d_repack);
     for (k = 0; k < SG_MAX_DIMS; k++) {
         cudaFree(g->d_chains[k]);
         cudaFree(g->d_seg[k]);
@@ -240,7 +246,9 @@ static void leave(sg_grid *g, int prev)
 static int materialize(sg_grid *g)
 {
     const sg_layout *L = &g->L;
-    uint32_t *leaf = NULL;
+    uint32_t *prefix = NULL;
+    sg_repack *rp = NULL;
+    int64_t nprefix = 0;
     int k, r;
     if (g->dev >= 0) return SG_OK;
     CU(cudaGetDevice(&g->dev), "cudaGetDevice");
@@ -248,14 +256,26 @@ static int materialize(sg_grid *g)
     CU(cudaMemset(g->d_alpha, 0, (size_t)L->Npad * 4), "cudaMemset");
     if ((r = dev_alloc(g, (void **)&g->d_err, 16, "error flag")) != SG_OK) goto bad;
     CU(cudaMemset(g->d_err, 0, 16), "cudaMemset");
-    if ((r = sg_layout_dfs_offsets(L, &leaf)) != SG_OK) {
-        fail(r, "building the evaluation order table");
+    if ((r = sg_layout_eval_tables(L, &prefix, &nprefix, &rp)) != SG_OK) {
+        fail(r, "building the evaluation layout tables");
         goto bad;
     }
-    if ((r = dev_alloc(g, (void **)&g->d_leaf, L->S * 4, "evaluation table")) != SG_OK) goto bad;
-    CU(cudaMemcpy(g->d_leaf, leaf, (size_t)L->S * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
-    free(leaf);
-    leaf = NULL;
+    for (k = 0; k < L->n; k++) {
+        sg_eval_shape sh;
+        sg_layout_eval_shape(L, k, &sh);
+        g->blk[k] = sh.aoff[sh.amax + 1];
+    }
+    if ((r = dev_alloc(g, (void **)&g->d_blk, L->N * 4, "block layout")) != SG_OK) goto bad;
+    if ((r = dev_alloc(g, (void **)&g->d_prefix, nprefix * 4, "block bases")) != SG_OK) goto bad;
+    if ((r = dev_alloc(g, (void **)&g->d_repack, L->S * (int64_t)sizeof(sg_repack), "repack table")) != SG_OK)
+        goto bad;
+    CU(cudaMemcpy(g->d_prefix, prefix, (size_t)nprefix * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
+    CU(cudaMemcpy(g->d_repack, rp, (size_t)L->S * sizeof(sg_repack), cudaMemcpyHostToDevice), "cudaMemcpy");
+    free(prefix);
+    free(rp);
+    prefix = NULL;
+    rp = NULL;
+    g->eval_dirty = 1;
     for (k = 0; k < L->d; k++) {
         sg_chain *ch = NULL;
         uint32_t *seg = NULL;
@@ -296,13 +316,16 @@ static int materialize(sg_grid *g)
     }
     return SG_OK;
 bad:
-    free(leaf);
+    free(prefix);
+    free(rp);
     free_device(g);
     memset(g->d_chains, 0, sizeof(g->d_chains));
     memset(g->d_seg, 0, sizeof(g->d_seg));
     g->d_alpha = NULL;
     g->d_work = NULL;
-    g->d_leaf = NULL;
+    g->d_blk = NULL;
+    g->d_prefix = NULL;
+    g->d_repack = NULL;
     g->d_err = NULL;
     g->d_scratch = g->d_io = NULL;
     g->scratch_bytes = g->io_bytes = g->dev_bytes = 0;
@@ -338,7 +361,7 @@ SG_API int sg_set_values(sg_grid *g, const float *values)
         (r = copy_groups(g, g->d_alpha, values, 1, cudaMemcpyHostToDevice, 0)) == SG_OK) {
         cudaError_t e = cudaStreamSynchronize(0);
         if (e != cudaSuccess) r = cuda_fail(e, "sg_set_values");
-        else g->has_values = 1;
+        else g->has_values = 1, g->eval_dirty = 1;
     }
     leave(g, prev);
     return r;
@@ -351,7 +374,7 @@ SG_API int sg_set_values_device(sg_grid *g, const float *values, void *stream)
     if ((r = enter(g, &prev)) != SG_OK) return r;
     if ((r = materialize(g)) == SG_OK &&
         (r = copy_groups(g, g->d_alpha, values, 1, cudaMemcpyDeviceToDevice, (cudaStream_t)stream)) == SG_OK)
-        g->has_values = 1;
+        g->has_values = 1, g->eval_dirty = 1;
     leave(g, prev);
     return r;
 }
@@ -454,6 +477,7 @@ SG_API int sg_hierarchize_async(sg_grid *g, void *stream)
     if ((r = enter(g, &prev)) != SG_OK) return r;
     mark(g, SG_PHASE_HIERARCHIZE, 0, (cudaStream_t)stream);
     r = hierarchize_on(g, (cudaStream_t)stream);
+    g->eval_dirty = 1;
     mark(g, SG_PHASE_HIERARCHIZE, 1, (cudaStream_t)stream);
     leave(g, prev);
     return r;
@@ -510,11 +534,17 @@ static int evaluate_on(sg_grid *g, const float *coords, float *out, int64_t m, c
 {
     sg_eval_plan p;
     int e, k;
-    p.alpha = g->d_alpha;
-    p.leaf = g->d_leaf;
+    if (g->eval_dirty) {
+        if ((e = sgk_repack(g->d_alpha, g->d_blk, g->d_repack, g->L.S, st)) != cudaSuccess)
+            return cuda_fail((cudaError_t)e, "repacking surpluses");
+        g->eval_dirty = 0;
+    }
+    p.alpha = g->d_blk;
+    p.prefix_base = g->d_prefix;
     p.d = g->L.d;
     p.n = g->L.n;
     for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < g->L.d ? g->L.lim[k] : 0;
+    for (k = 0; k < SG_MAX_LEVELS; k++) p.blk[k] = g->blk[k];
     p.ppt = eval_ppt(g);
     if (g->opt[SG_OPT_EVAL_SORT] && m > 1) {
         const int64_t sort_b = (sgk_sort_scratch_bytes(m, p.d) + 255) & ~(int64_t)255;
@@ -598,7 +628,7 @@ SG_API int sg_sample_function(sg_grid *g, int fn, const double *params, int np, 
         if ((e = sgk_sample(&g->L, fn, params, np, g->d_alpha, stream)) != cudaSuccess)
             r = cuda_fail((cudaError_t)e, "sg_sample_function");
         else
-            g->has_values = 1;
+            g->has_values = 1, g->eval_dirty = 1;
     }
     leave(g, prev);
     return r;

@@ -22,9 +22,9 @@ EVAL_RTOL_NORM = 1e-5
 EVAL_ATOL = 2e-7
 
 
-def _grid(d, n, lim=None, **opt):
+def _grid(d, n, lim=None, opt=None):
     g = sg.Grid(d, n, lim)
-    for k, v in opt.items():
+    for k, v in (opt or {}).items():
         g.set_option(k, v)
     return g
 
@@ -77,7 +77,7 @@ SHAPES = [
 @pytest.mark.parametrize("kernel", [0, 2])
 def test_hierarchize_fp32_bitexact(cuda, d, n, lim, kernel):
     o = Oracle(d, n, lim)
-    g = _grid(d, n, lim, **{sg.SG_OPT_HIER_KERNEL: kernel})
+    g = _grid(d, n, lim, {sg.SG_OPT_HIER_KERNEL: kernel})
     v = inputs.uniform01(d * 31 + n, g.num_points) * 2 - 1
     g.set_values(v)
     g.hierarchize()
@@ -90,7 +90,7 @@ def test_hierarchize_fp32_bitexact(cuda, d, n, lim, kernel):
 @pytest.mark.parametrize("kernel", [0, 2])
 def test_hierarchize_fp64_matches_fp64_oracle(cuda, d, n, lim, kernel):
     o = Oracle(d, n, lim)
-    g = _grid(d, n, lim, **{sg.SG_OPT_HIER_KERNEL: kernel, sg.SG_OPT_HIER_PRECISION: sg.SG_HIER_FP64})
+    g = _grid(d, n, lim, {sg.SG_OPT_HIER_KERNEL: kernel, sg.SG_OPT_HIER_PRECISION: sg.SG_HIER_FP64})
     v = inputs.uniform01(d * 17 + n, g.num_points) * 2 - 1
     g.set_values(v)
     g.hierarchize()
@@ -103,7 +103,7 @@ def test_hierarchize_fp64_matches_fp64_oracle(cuda, d, n, lim, kernel):
 @pytest.mark.parametrize("ppt", [1, 2])
 def test_evaluate_vs_fp64_oracle(cuda, d, n, lim, ppt):
     o = Oracle(d, n, lim)
-    g = _grid(d, n, lim, **{sg.SG_OPT_EVAL_PPT: ppt})
+    g = _grid(d, n, lim, {sg.SG_OPT_EVAL_PPT: ppt})
     vals = inputs.grid_values(g, inputs.f_gauss)
     g.set_values(vals)
     g.hierarchize()
@@ -188,6 +188,25 @@ def test_device_bijection(cuda):
         for i in range(0, g.num_points, max(1, g.num_points // 300)):
             a, b = o.idx2gp(i)
             assert np.array_equal(lvh[i], a) and np.array_equal(ixh[i], b)
+
+
+@pytest.mark.parametrize("fn,params,host", [
+    (0, (), inputs.f_reference), (1, (), inputs.f_prod4), (2, (), inputs.f_gauss),
+    (3, (0.3, 50.0), inputs.f_bump), (4, None, None)])
+def test_sample_function_on_device(cuda, fn, params, host):
+    d, n, lim = 4, 7, [6, 3, 6, 2]
+    g = sg.Grid(d, n, lim)
+    if fn == 4:
+        coef = (inputs.uniform01(3, 3 * d).astype(np.float64) * 2 - 1).reshape(d, 3)
+        params = coef.reshape(-1)
+        host = lambda X: inputs.f_quad(X, coef)  # noqa: E731
+    g.sample_function(fn, params)
+    got = g.get_values()
+    want = host(inputs.grid_coordinates(g)).astype(np.float32)
+    # FP64 evaluation order and libm may differ in the last FP64 bits: allow
+    # one FP32 ulp after the single rounding
+    ulp = np.spacing(np.abs(want).astype(np.float32))
+    assert np.all(np.abs(got - want) <= ulp), np.max(np.abs(got - want) / ulp)
 
 
 def test_errors_on_gpu(cuda):
