@@ -1,0 +1,5 @@
+/* Evaluation kernels for d = 1 and 2 (see eval_impl.cuh). */
+#include "eval_impl.cuh"
+
+template int eval_launch<1>(const EvalArgs &, int, void *);
+template int eval_launch<2>(const EvalArgs &, int, void *);

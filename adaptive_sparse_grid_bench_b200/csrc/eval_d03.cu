@@ -1,0 +1,5 @@
+/* Evaluation kernels for d = 3 and 4 (see eval_impl.cuh). */
+#include "eval_impl.cuh"
+
+template int eval_launch<3>(const EvalArgs &, int, void *);
+template int eval_launch<4>(const EvalArgs &, int, void *);

@@ -1,0 +1,5 @@
+/* Evaluation kernels for d = 5 and 6 (see eval_impl.cuh). */
+#include "eval_impl.cuh"
+
+template int eval_launch<5>(const EvalArgs &, int, void *);
+template int eval_launch<6>(const EvalArgs &, int, void *);

@@ -1,0 +1,5 @@
+/* Evaluation kernels for d = 7 and 8 (see eval_impl.cuh). */
+#include "eval_impl.cuh"
+
+template int eval_launch<7>(const EvalArgs &, int, void *);
+template int eval_launch<8>(const EvalArgs &, int, void *);

@@ -1,0 +1,5 @@
+/* Evaluation kernels for d = 15 and 16 (see eval_impl.cuh). */
+#include "eval_impl.cuh"
+
+template int eval_launch<15>(const EvalArgs &, int, void *);
+template int eval_launch<16>(const EvalArgs &, int, void *);

@@ -1,0 +1,420 @@
+/*
+ * Evaluation kernels for sm_100a (instantiated per dimension in eval_d*.cu).
+ *
+ * Reference algorithm: evaluate0 in adaptive_sparse_grid_bench.c:1237-1274
+ * (definition) and evaluate5 (c:1558-1688): for a query point x,
+ *     u(x) = sum over subspaces l of  a[off(l) + idx(x, l)] * prod_k hat_k
+ * with t_k = floor(x_k 2^l_k), idx(x, l) = row-major (t_0, ..., t_{d-1}) over
+ * the subspace (dim 0 most significant) and hat_k = 1 - |x_k 2^(l_k+1) - (2t_k+1)|.
+ *
+ * B200 design.  One thread owns P query points; every warp walks the same
+ * depth-first tree over the level vectors of the prefix dims 0..d-4 (each
+ * dim's level ascending, sum(l) <= n-1, l_k <= limits[k]), so control flow is
+ * uniform across the warp and partial products / partial cell indices are
+ * shared by all subspaces below a node.  Below a prefix cell the walk reads
+ * one block: every subspace of the three innermost dims (C = d-3, A = d-2,
+ * B = d-1), stored contiguously in the block layout (sg_layout.h) with dim
+ * B's levels as a 1-D heap.  The surplus of (c, a, b) sits at
+ *     base + coff(c) + t_c sub(R-c) + aoff(a) + t_a plen(a) + (2^b - 1 + t_b):
+ *   - blocks follow each other in walk order, so the block base is a running
+ *     counter plus one multiply-add per point (no table);
+ *   - 2^b - 1 + t_b and the hats of dims A, B (and C for small budgets) are
+ *     precomputed per point in registers, so each subspace costs one add,
+ *     one gather and one FMA;
+ *   - in regular grids, blocks of budget R <= kRF run fully unrolled; larger
+ *     blocks loop over their planes and run each plane's 2-D sub-block fully
+ *     unrolled behind a jump table; a generic loop covers limits on the
+ *     innermost dims, budgets >= kNB and d = 1;
+ *   - per prefix dim the walk keeps three values per point: the fractional
+ *     part y = frac(x 2^l) (next level: doubling, exact in FP32), the cell
+ *     index of the prefix (next level: 2*ix + bit) and the parent's product;
+ *   - block sums of one prefix node are accumulated with FMAs and the node's
+ *     total enters a Kahan-compensated accumulator.
+ * Query points are put in spatial (Morton) order beforehand so the 32 points
+ * of a warp share cells of the coarse subspaces and the gathers of a warp
+ * touch few sectors; the grid is then served from L1/L2.
+ */
+#ifndef SG_EVAL_IMPL_CUH
+#define SG_EVAL_IMPL_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "eval_args.h"
+
+namespace sgeval {
+
+constexpr int kThreads = 256;
+constexpr int kNB = 10; /* 2-D sub-blocks of budget r < kNB run fully unrolled */
+constexpr int kRF = 3;  /* 3-D blocks of budget R <= kRF run fully unrolled    */
+constexpr int kTB = 15; /* T = floor(x 2^15) holds the cells of levels 0..15   */
+
+__device__ __forceinline__ void kahan_add(float &s, float &c, float v)
+{
+    const float y = __fsub_rn(v, c);
+    const float t = __fadd_rn(s, y);
+    c = __fsub_rn(__fsub_rn(t, s), y);
+    s = t;
+}
+
+/* hat at the current level from the fractional part y = frac(x 2^l) */
+__device__ __forceinline__ float hat_of(float y)
+{
+    return 1.0f - fabsf(fmaf(2.0f, y, -1.0f));
+}
+
+/* next level: y <- frac(2y) (exact), returns floor(2y) */
+__device__ __forceinline__ uint32_t step_y(float &y)
+{
+    const float y2 = y + y;
+    const bool b = y2 >= 1.0f;
+    y = b ? y2 - 1.0f : y2;
+    return (uint32_t)b;
+}
+
+/* Per-point values of the three innermost dims. */
+template <int P>
+struct Inner {
+    float hB[P][kNB];     /* hat of dim B at level b                 */
+    uint32_t cB[P][kNB];  /* heap index 2^b - 1 + t_b of dim B       */
+    float hA[P][kNB];     /* hat of dim A at level a                 */
+    float hC[P][kRF + 1]; /* hat of dim C at level c                 */
+    uint32_t TA[P];       /* floor(x_A 2^15): t_a = TA >> (15 - a)   */
+    uint32_t TC[P];       /* floor(x_C 2^15)                         */
+};
+
+/* Regular-grid shapes (all innermost limits >= n-1). */
+__host__ __device__ constexpr uint32_t plen_reg(int r, int a) { return (2u << (r - a)) - 1u; }
+__host__ __device__ constexpr uint32_t aoff_reg(int r, int a)
+{
+    uint32_t o = 0;
+    for (int q = 0; q < a; ++q) o += (1u << q) * plen_reg(r, q);
+    return o;
+}
+__host__ __device__ constexpr uint32_t blk2_reg(int r) { return aoff_reg(r, r + 1); }
+__host__ __device__ constexpr uint32_t coff_reg(int R, int c)
+{
+    uint32_t o = 0;
+    for (int q = 0; q < c; ++q) o += (1u << q) * blk2_reg(R - q);
+    return o;
+}
+
+/* 2-D sub-block of budget r: rows a = 0..r, row a holds 2^a poles of r-a+1
+ * levels.  Returns sum_a hA[a] sum_b hB[b] alpha[...]. */
+template <int r, int P>
+__device__ __forceinline__ void block2_fixed(const float *__restrict__ alpha, const uint32_t (&base)[P],
+                                             const Inner<P> &in, float (&s)[P])
+{
+#pragma unroll
+    for (int a = 0; a <= r; ++a) {
+        uint32_t rb[P];
+        float sr[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            rb[p] = base[p] + aoff_reg(r, a) + (in.TA[p] >> (kTB - a)) * plen_reg(r, a);
+            sr[p] = 0.0f;
+        }
+#pragma unroll
+        for (int b = 0; b <= r - a; ++b)
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                sr[p] = fmaf(in.hB[p][b], __ldg(alpha + rb[p] + in.cB[p][b]), sr[p]);
+#pragma unroll
+        for (int p = 0; p < P; ++p) s[p] = (a == 0) ? in.hA[p][0] * sr[p] : fmaf(in.hA[p][a], sr[p], s[p]);
+    }
+}
+
+/* planes C..R of a fully unrolled 3-D block of budget R */
+template <int R, int C, int P>
+__device__ __forceinline__ void block3_planes(const float *__restrict__ alpha, const uint32_t (&base)[P],
+                                              const Inner<P> &in, float (&s)[P])
+{
+    uint32_t sb[P];
+    float s2[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) sb[p] = base[p] + coff_reg(R, C) + (in.TC[p] >> (kTB - C)) * blk2_reg(R - C);
+    block2_fixed<R - C, P>(alpha, sb, in, s2);
+#pragma unroll
+    for (int p = 0; p < P; ++p) s[p] = (C == 0) ? in.hC[p][0] * s2[p] : fmaf(in.hC[p][C], s2[p], s[p]);
+    if constexpr (C < R) block3_planes<R, C + 1, P>(alpha, base, in, s);
+}
+
+/* Generic sub-block of budget r (limits, r >= kNB): runtime loops. */
+template <int P>
+__device__ __forceinline__ void block2_generic(const float *__restrict__ alpha, int r, int limA, int limB,
+                                               const float (&xA)[P], const float (&xB)[P], bool hasA,
+                                               const uint32_t (&base)[P], float (&s)[P])
+{
+    const int amax = min(r, limA);
+    uint32_t aoff = 0;
+    float yA[P];
+    uint32_t tA[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        yA[p] = xA[p];
+        tA[p] = 0;
+        s[p] = 0.0f;
+    }
+    for (int a = 0; a <= amax; ++a) {
+        if (a) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) tA[p] = 2 * tA[p] + step_y(yA[p]);
+        }
+        const int rl = min(r - a, limB) + 1;
+        const uint32_t plen = (1u << rl) - 1u;
+        float yB[P], sr[P];
+        uint32_t tB[P], rb[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            yB[p] = xB[p];
+            tB[p] = 0;
+            sr[p] = 0.0f;
+            rb[p] = base[p] + aoff + tA[p] * plen;
+        }
+        for (int b = 0; b < rl; ++b) {
+            if (b) {
+#pragma unroll
+                for (int p = 0; p < P; ++p) tB[p] = 2 * tB[p] + step_y(yB[p]);
+            }
+#pragma unroll
+            for (int p = 0; p < P; ++p)
+                sr[p] = fmaf(hat_of(yB[p]), __ldg(alpha + rb[p] + (1u << b) - 1u + tB[p]), sr[p]);
+        }
+#pragma unroll
+        for (int p = 0; p < P; ++p) s[p] = fmaf(hasA ? hat_of(yA[p]) : 1.0f, sr[p], s[p]);
+        aoff += (1u << a) * plen;
+    }
+}
+
+/* Sub-block of budget r: unrolled (regular, r < kNB) or generic. */
+template <int D, int P>
+__device__ __forceinline__ void block2_any(const EvalArgs &A, int r, const Inner<P> &in, const float (&xA)[P],
+                                           const float (&xB)[P], const uint32_t (&base)[P], float (&s)[P])
+{
+    if (D >= 2 && A.regular) {
+        switch (r) {
+#define SG_BLK2(RR) \
+    case RR: block2_fixed<RR, P>(A.alpha, base, in, s); return;
+            SG_BLK2(0) SG_BLK2(1) SG_BLK2(2) SG_BLK2(3) SG_BLK2(4)
+            SG_BLK2(5) SG_BLK2(6) SG_BLK2(7) SG_BLK2(8) SG_BLK2(9)
+#undef SG_BLK2
+        default: break;
+        }
+    }
+    block2_generic<P>(A.alpha, r, D >= 2 ? A.lim[D >= 2 ? D - 2 : 0] : 0, A.lim[D - 1], xA, xB, D >= 2, base, s);
+}
+
+/* Sum over the block of budget R at `base` for every point. */
+template <int D, int P>
+__device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<P> &in, const float (&xC)[P],
+                                          const float (&xA)[P], const float (&xB)[P], const uint32_t (&base)[P],
+                                          float (&s)[P])
+{
+    if constexpr (D >= 3) {
+        if (A.regular && R <= kRF) {
+            switch (R) {
+            case 0: block3_planes<0, 0, P>(A.alpha, base, in, s); return;
+            case 1: block3_planes<1, 0, P>(A.alpha, base, in, s); return;
+            case 2: block3_planes<2, 0, P>(A.alpha, base, in, s); return;
+            default: block3_planes<kRF, 0, P>(A.alpha, base, in, s); return;
+            }
+        }
+    }
+    /* plane loop; dim C is absent (limit 0) for d < 3 */
+    const int cmax = D >= 3 ? min(R, A.lim[D >= 3 ? D - 3 : 0]) : 0;
+    uint32_t coff = 0;
+    float yC[P];
+    uint32_t tC[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        yC[p] = xC[p];
+        tC[p] = 0;
+        s[p] = 0.0f;
+    }
+    for (int c = 0; c <= cmax; ++c) {
+        if (c) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) tC[p] = 2 * tC[p] + step_y(yC[p]);
+        }
+        const uint32_t sub = A.blk2[R - c];
+        uint32_t sb[P];
+        float s2[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) sb[p] = base[p] + coff + tC[p] * sub;
+        block2_any<D, P>(A, R - c, in, xA, xB, sb, s2);
+#pragma unroll
+        for (int p = 0; p < P; ++p) s[p] = fmaf(D >= 3 ? hat_of(yC[p]) : 1.0f, s2[p], s[p]);
+        coff += (1u << c) * sub;
+    }
+}
+
+/* Walk over prefix dim K (K <= D-4); children of depth D-4 are blocks. */
+template <int D, int K, int P>
+struct Walk {
+    static __device__ __forceinline__ void run(const EvalArgs &A, const float *sx, int tid, int budget,
+                                               uint32_t &cur, const Inner<P> &in, const float (&xC)[P],
+                                               const float (&xA)[P], const float (&xB)[P], const float (&pin)[P],
+                                               const uint32_t (&ixin)[P], float (&sum)[P], float (&comp)[P])
+    {
+        const int lmax = min(A.lim[K], budget);
+        float y[P], acc[P];
+        uint32_t ix[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            y[p] = sx[(K * P + p) * kThreads + tid];
+            ix[p] = ixin[p];
+            acc[p] = 0.0f;
+        }
+        for (int l = 0; l <= lmax; ++l) {
+            if (l) {
+#pragma unroll
+                for (int p = 0; p < P; ++p) ix[p] = 2 * ix[p] + step_y(y[p]);
+            }
+            float pn[P];
+#pragma unroll
+            for (int p = 0; p < P; ++p) pn[p] = pin[p] * hat_of(y[p]);
+            if constexpr (K == D - 4) {
+                const int R = budget - l;
+                const uint32_t blk = A.blk3[R];
+                uint32_t base[P];
+                float s[P];
+#pragma unroll
+                for (int p = 0; p < P; ++p) base[p] = cur + ix[p] * blk;
+                cur += blk << (A.nm1 - R);
+                block_sum<D, P>(A, R, in, xC, xA, xB, base, s);
+#pragma unroll
+                for (int p = 0; p < P; ++p) acc[p] = fmaf(pn[p], s[p], acc[p]);
+            } else {
+                Walk<D, K + 1, P>::run(A, sx, tid, budget - l, cur, in, xC, xA, xB, pn, ix, sum, comp);
+            }
+        }
+        if constexpr (K == D - 4) {
+#pragma unroll
+            for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], acc[p]);
+        }
+    }
+};
+
+template <int D, int P>
+__global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const EvalArgs A)
+{
+    constexpr int NPX = D >= 4 ? D - 3 : 1; /* prefix coordinates kept in shared memory */
+    __shared__ float sx[NPX * P * kThreads];
+    const int tid = threadIdx.x;
+    const int64_t warp = (blockIdx.x * (int64_t)kThreads + tid) >> 5;
+    const int lane = tid & 31;
+    const int64_t first = warp * (32 * P) + lane;
+
+    float xC[P], xA[P], xB[P];
+    bool valid[P], nan_in[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int64_t i = first + 32 * p;
+        float x[D];
+        valid[p] = i < A.num_evals;
+        nan_in[p] = false;
+        bool inside = true;
+#pragma unroll
+        for (int k = 0; k < D; ++k) {
+            const float v = valid[p] ? A.coords[i * D + k] : 0.0f;
+            nan_in[p] |= (v != v);
+            inside &= (v >= 0.0f) && (v < 1.0f);
+            x[k] = v;
+        }
+        /* outside [0,1)^d every basis function is 0: walk at x = 0 (always
+         * in range) and write 0 (NaN for NaN input) instead */
+        if (!inside) {
+#pragma unroll
+            for (int k = 0; k < D; ++k) x[k] = 0.0f;
+        }
+        valid[p] = valid[p] && inside;
+#pragma unroll
+        for (int k = 0; k + 3 < D; ++k) sx[(k * P + p) * kThreads + tid] = x[k];
+        xC[p] = D >= 3 ? x[D >= 3 ? D - 3 : 0] : 0.0f;
+        xA[p] = D >= 2 ? x[D >= 2 ? D - 2 : 0] : 0.0f;
+        xB[p] = x[D - 1];
+    }
+
+    Inner<P> in;
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        float y = xB[p];
+        uint32_t t = 0;
+#pragma unroll
+        for (int j = 0; j < kNB; ++j) {
+            if (j) t = 2 * t + step_y(y);
+            in.hB[p][j] = hat_of(y);
+            in.cB[p][j] = ((1u << j) - 1u) + t;
+        }
+        in.TA[p] = (uint32_t)(xA[p] * (float)(1u << kTB));
+        y = xA[p];
+#pragma unroll
+        for (int j = 0; j < kNB; ++j) {
+            if (j) (void)step_y(y);
+            in.hA[p][j] = hat_of(y);
+        }
+        in.TC[p] = (uint32_t)(xC[p] * (float)(1u << kTB));
+        y = xC[p];
+#pragma unroll
+        for (int j = 0; j <= kRF; ++j) {
+            if (j) (void)step_y(y);
+            in.hC[p][j] = hat_of(y);
+        }
+    }
+
+    float sum[P], comp[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        sum[p] = 0.0f;
+        comp[p] = 0.0f;
+    }
+    uint32_t cur = 0;
+    if constexpr (D >= 4) {
+        float pin[P];
+        uint32_t ix[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            pin[p] = 1.0f;
+            ix[p] = 0;
+        }
+        Walk<D, 0, P>::run(A, sx, tid, A.nm1, cur, in, xC, xA, xB, pin, ix, sum, comp);
+    } else {
+        uint32_t base[P];
+        float s[P];
+#pragma unroll
+        for (int p = 0; p < P; ++p) base[p] = 0;
+        block_sum<D, P>(A, A.nm1, in, xC, xA, xB, base, s);
+#pragma unroll
+        for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], s[p]);
+    }
+
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        const int64_t i = first + 32 * p;
+        if (i < A.num_evals) {
+            const float r = valid[p] ? __fsub_rn(sum[p], comp[p]) : (nan_in[p] ? __int_as_float(0x7fc00000) : 0.0f);
+            A.out[A.perm ? A.perm[i] : i] = r;
+        }
+    }
+}
+
+template <int D, int P>
+int launch_eval(const EvalArgs &A, void *stream)
+{
+    const int64_t per_block = (int64_t)kThreads * P;
+    const int64_t blocks = (A.num_evals + per_block - 1) / per_block;
+    if (blocks > 0x7fffffff) return cudaErrorInvalidValue;
+    k_evaluate<D, P><<<(unsigned)blocks, kThreads, 0, (cudaStream_t)stream>>>(A);
+    return cudaGetLastError();
+}
+
+} // namespace sgeval
+
+template <int D>
+int eval_launch(const EvalArgs &A, int ppt, void *stream)
+{
+    if (ppt == 1) return sgeval::launch_eval<D, 1>(A, stream);
+    return sgeval::launch_eval<D, 2>(A, stream);
+}
+
+#endif

@@ -32,299 +32,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "eval_args.h"
 #include "sg_kernels.h"
 
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kNB = 12; /* blocks with level budget R < kNB run fully unrolled */
-constexpr int kTB = 15; /* T = floor(x 2^15) holds the cells of levels 0..15  */
-
-struct EvalArgs {
-    const float *__restrict__ alpha;          /* block layout                 */
-    const uint32_t *__restrict__ prefix_base; /* one block base per prefix    */
-    const float *__restrict__ coords;
-    const int32_t *__restrict__ perm;
-    float *__restrict__ out;
-    int64_t num_evals;
-    int nm1;                                  /* n - 1                        */
-    int regular2;                             /* last two dims unrestricted   */
-    int lim[SG_MAX_DIMS];
-    uint32_t blk[SG_MAX_LEVELS];              /* block size per budget R      */
-};
-
-__device__ __forceinline__ void kahan_add(float &s, float &c, float v)
-{
-    const float y = __fsub_rn(v, c);
-    const float t = __fadd_rn(s, y);
-    c = __fsub_rn(__fsub_rn(t, s), y);
-    s = t;
-}
-
-/* hat at the current level from the fractional part y = frac(x 2^l) */
-__device__ __forceinline__ float hat_of(float y)
-{
-    return 1.0f - fabsf(fmaf(2.0f, y, -1.0f));
-}
-
-/* next level: y <- frac(2y), t <- 2t + floor(2y); exact in FP32 */
-__device__ __forceinline__ void step_level(float &y, uint32_t &t)
-{
-    const float y2 = y + y;
-    const bool b = y2 >= 1.0f;
-    y = b ? y2 - 1.0f : y2;
-    t = (t << 1) | (uint32_t)b;
-}
-
-/* Per-point values of the two innermost dims (A = d-2, B = d-1). */
-template <int P>
-struct Inner {
-    float hB[P][kNB];    /* hat of dim B at level b                      */
-    uint32_t cB[P][kNB]; /* heap index 2^b - 1 + t_b of dim B            */
-    float hA[P][kNB];    /* hat of dim A at level a                      */
-    uint32_t TA[P];      /* floor(x_A 2^15): t_a = TA >> (15 - a)        */
-};
-
-__host__ __device__ constexpr uint32_t aoff_reg(int R, int a)
-{
-    uint32_t o = 0;
-    for (int q = 0; q < a; ++q) o += (1u << q) * ((2u << (R - q)) - 1u);
-    return o;
-}
-
-/* One block of budget R of a grid whose last two dims are unrestricted:
- * rows a = 0..R, row a holds 2^a poles of R-a+1 levels.  Fully unrolled:
- * one add, one gather and one FMA per subspace and point. */
-template <int R, int P>
-__device__ __forceinline__ void block_fixed(const float *__restrict__ alpha, const uint32_t (&base)[P],
-                                            const Inner<P> &in, float (&s)[P])
-{
-#pragma unroll
-    for (int a = 0; a <= R; ++a) {
-        const uint32_t plen = (2u << (R - a)) - 1u;
-        const uint32_t ao = aoff_reg(R, a);
-        uint32_t rb[P];
-        float sr[P];
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-            rb[p] = base[p] + ao + (in.TA[p] >> (kTB - a)) * plen;
-            sr[p] = 0.0f;
-        }
-#pragma unroll
-        for (int b = 0; b <= R - a; ++b)
-#pragma unroll
-            for (int p = 0; p < P; ++p)
-                sr[p] = fmaf(in.hB[p][b], __ldg(alpha + rb[p] + in.cB[p][b]), sr[p]);
-#pragma unroll
-        for (int p = 0; p < P; ++p) s[p] = fmaf(in.hA[p][a], sr[p], s[p]);
-    }
-}
-
-template <int R, int P>
-__device__ __forceinline__ bool block_dispatch(int r, const float *__restrict__ alpha, const uint32_t (&base)[P],
-                                               const Inner<P> &in, float (&s)[P])
-{
-    if (r == R) {
-        block_fixed<R, P>(alpha, base, in, s);
-        return true;
-    }
-    if constexpr (R + 1 < kNB) return block_dispatch<R + 1, P>(r, alpha, base, in, s);
-    return false;
-}
-
-/* Any block: runtime loops, hats stepped level by level (limits on the last
- * two dims, budgets R >= kNB, and d = 1 where dim A is absent). */
-template <int D, int P>
-__device__ __forceinline__ void block_generic(const EvalArgs &A, int R, const float (&x)[P][D],
-                                              const uint32_t (&base)[P], float (&s)[P])
-{
-    const int limA = D >= 2 ? A.lim[D - 2] : 0;
-    const int limB = A.lim[D - 1];
-    const int amax = min(R, limA);
-    uint32_t aoff = 0;
-    float yA[P];
-    uint32_t tA[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-        yA[p] = D >= 2 ? x[p][D >= 2 ? D - 2 : 0] : 0.0f;
-        tA[p] = 0;
-    }
-    for (int a = 0; a <= amax; ++a) {
-        if (a) {
-#pragma unroll
-            for (int p = 0; p < P; ++p) step_level(yA[p], tA[p]);
-        }
-        const int rl = min(R - a, limB) + 1;
-        const uint32_t plen = (1u << rl) - 1u;
-        float yB[P], sr[P];
-        uint32_t tB[P], rb[P];
-#pragma unroll
-        for (int p = 0; p < P; ++p) {
-            yB[p] = x[p][D - 1];
-            tB[p] = 0;
-            sr[p] = 0.0f;
-            rb[p] = base[p] + aoff + tA[p] * plen;
-        }
-        for (int b = 0; b < rl; ++b) {
-            if (b) {
-#pragma unroll
-                for (int p = 0; p < P; ++p) step_level(yB[p], tB[p]);
-            }
-#pragma unroll
-            for (int p = 0; p < P; ++p)
-                sr[p] = fmaf(hat_of(yB[p]), __ldg(A.alpha + rb[p] + (1u << b) - 1u + tB[p]), sr[p]);
-        }
-#pragma unroll
-        for (int p = 0; p < P; ++p) s[p] = fmaf(D >= 2 ? hat_of(yA[p]) : 1.0f, sr[p], s[p]);
-        aoff += (1u << a) * plen;
-    }
-}
-
-/* Depth-first walk over the prefix dims 0..D-3; at depth D-2 one block. */
-template <int D, int K, int P>
-struct Walk {
-    static __device__ __forceinline__ void run(const EvalArgs &A, int budget, int &pc, const float (&x)[P][D],
-                                               const Inner<P> &in, const float (&pin)[P],
-                                               const uint32_t (&iin)[P], float (&sum)[P], float (&comp)[P])
-    {
-        if constexpr (K >= D - 2) {
-            const int R = budget;
-            const uint32_t bb = __ldg(A.prefix_base + pc);
-            ++pc;
-            const uint32_t blk = A.blk[R];
-            uint32_t base[P];
-            float s[P];
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-                base[p] = bb + iin[p] * blk;
-                s[p] = 0.0f;
-            }
-            bool done = false;
-            if (D >= 2 && A.regular2) done = block_dispatch<0, P>(R, A.alpha, base, in, s);
-            if (!done) block_generic<D, P>(A, R, x, base, s);
-#pragma unroll
-            for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], pin[p] * s[p]);
-        } else {
-            const int lmax = min(A.lim[K], budget);
-            float y[P];
-            uint32_t t[P], J[P];
-#pragma unroll
-            for (int p = 0; p < P; ++p) {
-                y[p] = x[p][K];
-                t[p] = 0;
-                J[p] = iin[p];
-            }
-            for (int l = 0; l <= lmax; ++l) {
-                if (l) {
-#pragma unroll
-                    for (int p = 0; p < P; ++p) {
-                        step_level(y[p], t[p]);
-                        J[p] <<= 1;
-                    }
-                }
-                float pn[P];
-                uint32_t ix[P];
-#pragma unroll
-                for (int p = 0; p < P; ++p) {
-                    pn[p] = pin[p] * hat_of(y[p]);
-                    ix[p] = J[p] + t[p];
-                }
-                Walk<D, K + 1, P>::run(A, budget - l, pc, x, in, pn, ix, sum, comp);
-            }
-        }
-    }
-};
-
-template <int D, int P>
-__global__ void __launch_bounds__(kThreads) k_evaluate(const EvalArgs A)
-{
-    const int64_t warp = (blockIdx.x * (int64_t)kThreads + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const int64_t base = warp * (32 * P) + lane;
-
-    float x[P][D];
-    bool valid[P], nan_in[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-        const int64_t i = base + 32 * p;
-        valid[p] = i < A.num_evals;
-        nan_in[p] = false;
-        bool inside = true;
-#pragma unroll
-        for (int k = 0; k < D; ++k) {
-            const float v = valid[p] ? A.coords[i * D + k] : 0.0f;
-            nan_in[p] |= (v != v);
-            inside &= (v >= 0.0f) && (v < 1.0f);
-            x[p][k] = v;
-        }
-        /* outside [0,1)^d every basis function is 0: walk at x = 0 (always
-         * in range) and write 0 (NaN for NaN input) instead */
-        if (!inside) {
-#pragma unroll
-            for (int k = 0; k < D; ++k) x[p][k] = 0.0f;
-        }
-        valid[p] = valid[p] && inside;
-    }
-
-    Inner<P> in;
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-        float y = x[p][D - 1];
-        uint32_t t = 0;
-#pragma unroll
-        for (int j = 0; j < kNB; ++j) {
-            if (j) step_level(y, t);
-            in.hB[p][j] = hat_of(y);
-            in.cB[p][j] = ((1u << j) - 1u) + t;
-        }
-        const float xa = D >= 2 ? x[p][D >= 2 ? D - 2 : 0] : 0.0f;
-        in.TA[p] = (uint32_t)(xa * (float)(1u << kTB));
-        y = xa;
-#pragma unroll
-        for (int j = 0; j < kNB; ++j) {
-            if (j) y = (y + y >= 1.0f) ? y + y - 1.0f : y + y;
-            in.hA[p][j] = hat_of(y);
-        }
-    }
-
-    float pin[P], sum[P], comp[P];
-    uint32_t iin[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-        pin[p] = 1.0f;
-        iin[p] = 0;
-        sum[p] = 0.0f;
-        comp[p] = 0.0f;
-    }
-    int pc = 0;
-    Walk<D, 0, P>::run(A, A.nm1, pc, x, in, pin, iin, sum, comp);
-
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-        const int64_t i = base + 32 * p;
-        if (i < A.num_evals) {
-            const float r = valid[p] ? __fsub_rn(sum[p], comp[p]) : (nan_in[p] ? __int_as_float(0x7fc00000) : 0.0f);
-            A.out[A.perm ? A.perm[i] : i] = r;
-        }
-    }
-}
-
-template <int D, int P>
-int launch_eval(const EvalArgs &A, void *stream)
-{
-    const int64_t per_block = (int64_t)kThreads * P;
-    const int64_t blocks = (A.num_evals + per_block - 1) / per_block;
-    if (blocks > 0x7fffffff) return cudaErrorInvalidValue;
-    k_evaluate<D, P><<<(unsigned)blocks, kThreads, 0, (cudaStream_t)stream>>>(A);
-    return cudaGetLastError();
-}
-
-template <int D>
-int dispatch_ppt(const EvalArgs &A, int ppt, void *stream)
-{
-    if (ppt == 2) return launch_eval<D, 2>(A, stream);
-    return launch_eval<D, 1>(A, stream);
-}
 
 /* compact (group-aligned) layout -> block layout, one CTA per subspace */
 __global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
@@ -333,12 +46,13 @@ __global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
     for (int64_t q = blockIdx.x; q < nsub; q += gridDim.x) {
         const sg_repack r = rp[q];
         const int n = 1 << r.s;
-        const int ab = r.a + r.b;
+        const int ab = r.a + r.b, cab = r.c + ab;
         for (int e = threadIdx.x; e < n; e += blockDim.x) {
-            const uint32_t I = (uint32_t)e >> ab;
+            const uint32_t I = (uint32_t)e >> cab;
+            const uint32_t tc = ((uint32_t)e >> ab) & ((1u << r.c) - 1u);
             const uint32_t ta = ((uint32_t)e >> r.b) & ((1u << r.a) - 1u);
             const uint32_t tb = (uint32_t)e & ((1u << r.b) - 1u);
-            dst[r.dst + I * r.blk + ta * r.plen + tb] = src[r.src + e];
+            dst[r.dst + I * r.blk + tc * r.sub + ta * r.plen + tb] = src[r.src + e];
         }
     }
 }
@@ -476,19 +190,23 @@ int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm
     if (num_evals <= 0) return cudaSuccess;
     EvalArgs A;
     A.alpha = p->alpha;
-    A.prefix_base = p->prefix_base;
     A.coords = coords;
     A.perm = perm;
     A.out = out;
     A.num_evals = num_evals;
     A.nm1 = p->n - 1;
     for (int k = 0; k < SG_MAX_DIMS; ++k) A.lim[k] = k < p->d ? p->lim[k] : 0;
-    for (int r = 0; r < SG_MAX_LEVELS; ++r) A.blk[r] = p->blk[r];
-    A.regular2 = p->d >= 2 && p->lim[p->d - 2] >= p->n - 1 && p->lim[p->d - 1] >= p->n - 1;
+    for (int r = 0; r < SG_MAX_LEVELS; ++r) {
+        A.blk3[r] = p->blk3[r];
+        A.blk2[r] = p->blk2[r];
+    }
+    bool reg = true;
+    for (int k = p->d >= 3 ? p->d - 3 : 0; k < p->d; ++k) reg = reg && p->lim[k] >= p->n - 1;
+    A.regular = reg;
     const int ppt = p->ppt;
     switch (p->d) {
 #define SG_D(DD) \
-    case DD: return dispatch_ppt<DD>(A, ppt, stream);
+    case DD: return eval_launch<DD>(A, ppt, stream);
         SG_D(1) SG_D(2) SG_D(3) SG_D(4) SG_D(5) SG_D(6) SG_D(7) SG_D(8) SG_D(9) SG_D(10)
         SG_D(11) SG_D(12) SG_D(13) SG_D(14) SG_D(15) SG_D(16) SG_D(17) SG_D(18) SG_D(19)
         SG_D(20)

@@ -41,10 +41,10 @@ int sgk_narrow(const double *src, float *dst, int64_t n, void *stream);
 /* Evaluation. */
 typedef struct sg_eval_plan {
     const float *alpha;          /* device grid in the block layout          */
-    const uint32_t *prefix_base; /* device: block base of every prefix       */
     int d, n;
     int lim[SG_MAX_DIMS];
-    uint32_t blk[SG_MAX_LEVELS]; /* block size for each level budget R       */
+    uint32_t blk3[SG_MAX_LEVELS]; /* block size for each level budget R      */
+    uint32_t blk2[SG_MAX_LEVELS]; /* sub-block size for each level budget r  */
     int ppt;                     /* points per thread (1 or 2)               */
 } sg_eval_plan;
 

@@ -212,18 +212,17 @@ int sg_layout_chains(const sg_layout *L, int k, sg_chain **chains, int64_t *ncha
 
 /* ---- evaluation (block) layout ------------------------------------------ */
 
-void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh)
+static int lim_of(const sg_layout *L, int k) { return k >= 0 ? L->lim[k] : 0; }
+
+void sg_layout_eval_sub(const sg_layout *L, int r, sg_eval_sub *sh)
 {
-    const int d = L->d;
-    const int limA = d >= 2 ? L->lim[d - 2] : 0;
-    const int limB = L->lim[d - 1];
+    const int limA = lim_of(L, L->d - 2), limB = L->lim[L->d - 1];
     int a;
     uint32_t off = 0;
     memset(sh, 0, sizeof(*sh));
-    sh->R = R;
-    sh->amax = R < limA ? R : limA;
+    sh->amax = r < limA ? r : limA;
     for (a = 0; a <= sh->amax; a++) {
-        int rl = R - a < limB ? R - a : limB;
+        int rl = r - a < limB ? r - a : limB;
         sh->rowlen[a] = rl + 1;
         sh->aoff[a] = off;
         off += ((uint32_t)1 << a) * (((uint32_t)1 << (rl + 1)) - 1);
@@ -231,99 +230,90 @@ void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh)
     sh->aoff[sh->amax + 1] = off;
 }
 
-typedef struct {
-    const sg_layout *L;
-    uint32_t *base;
-    int64_t np, cap;
-    uint32_t next;
-    int err;
-} prefix_ctx;
-
-static void prefix_visit(void *vctx, int *lv, int sigma)
+void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh)
 {
-    prefix_ctx *c = (prefix_ctx *)vctx;
-    sg_eval_shape sh;
-    (void)lv;
-    if (c->err) return;
-    if (c->np == c->cap) {
-        c->cap = c->cap ? 2 * c->cap : 1024;
-        c->base = (uint32_t *)realloc(c->base, (size_t)c->cap * sizeof(uint32_t));
-        if (!c->base) { c->err = SG_ERR_NOMEM; return; }
+    const int limC = lim_of(L, L->d - 3);
+    int c;
+    uint32_t off = 0;
+    memset(sh, 0, sizeof(*sh));
+    sh->R = R;
+    sh->cmax = R < limC ? R : limC;
+    for (c = 0; c <= sh->cmax; c++) {
+        sg_eval_sub sub;
+        sg_layout_eval_sub(L, R - c, &sub);
+        sh->coff[c] = off;
+        off += ((uint32_t)1 << c) * sub.aoff[sub.amax + 1];
     }
-    sg_layout_eval_shape(c->L, c->L->n - 1 - sigma, &sh);
-    c->base[c->np++] = c->next;
-    c->next += ((uint32_t)1 << sigma) * sh.aoff[sh.amax + 1];
+    sh->coff[sh->cmax + 1] = off;
 }
 
-int sg_layout_eval_tables(const sg_layout *L, uint32_t **prefix_base, int64_t *nprefix,
-                          sg_repack **repack)
+int sg_layout_eval_tables(const sg_layout *L, sg_repack **repack, uint32_t *blk3, uint32_t *blk2)
 {
     const int d = L->d;
-    const int np_dims = d >= 2 ? d - 2 : 0; /* dims 0..d-3 form the prefix */
-    int dims[SG_MAX_DIMS], lv[SG_MAX_DIMS], i, s, k, R;
+    const int np_dims = d >= 3 ? d - 3 : 0; /* dims 0..d-4 form the prefix */
+    int lv[SG_MAX_DIMS], k, s, R;
     int64_t pos, r = 0;
-    int64_t cnt[SG_MAX_DIMS + 1][SG_MAX_LEVELS]; /* completions of dims k.. with sum <= R */
-    prefix_ctx c;
+    /* cnt[k][R]: level vectors over prefix dims k..np_dims-1 with sum <= R;
+     * sz[k][R]: total block-layout size of their blocks (all cells) */
+    int64_t cnt[SG_MAX_DIMS + 1][SG_MAX_LEVELS], sz[SG_MAX_DIMS + 1][SG_MAX_LEVELS];
     sg_repack *rp;
-    for (R = 0; R < L->n; R++) cnt[np_dims][R] = 1;
+    for (R = 0; R < L->n; R++) {
+        sg_eval_shape sh;
+        sg_eval_sub sub;
+        sg_layout_eval_shape(L, R, &sh);
+        sg_layout_eval_sub(L, R, &sub);
+        blk3[R] = sh.coff[sh.cmax + 1];
+        blk2[R] = sub.aoff[sub.amax + 1];
+        cnt[np_dims][R] = 1;
+        sz[np_dims][R] = blk3[R];
+    }
     for (k = np_dims - 1; k >= 0; k--)
         for (R = 0; R < L->n; R++) {
             int l;
-            int64_t v = 0;
-            for (l = 0; l <= R && l <= L->lim[k]; l++) v += cnt[k + 1][R - l];
+            int64_t v = 0, w = 0;
+            for (l = 0; l <= R && l <= L->lim[k]; l++) {
+                v += cnt[k + 1][R - l];
+                w += sz[k + 1][R - l] << l; /* 2^l cells of this dim */
+            }
             cnt[k][R] = v;
+            sz[k][R] = w;
         }
-    memset(&c, 0, sizeof(c));
-    memset(lv, 0, sizeof(lv));
-    c.L = L;
-    for (i = 0; i < np_dims; i++) dims[i] = i;
-    enum_levels(L, dims, np_dims, 0, L->n - 1, 0, lv, prefix_visit, &c);
-    if (c.err) {
-        free(c.base);
-        return c.err;
-    }
-    if ((int64_t)c.next != L->N) {
-        free(c.base);
-        return SG_ERR_STATE;
-    }
+    if (sz[0][L->n - 1] != L->N) return SG_ERR_STATE;
     rp = (sg_repack *)malloc((size_t)(L->S > 0 ? L->S : 1) * sizeof(sg_repack));
-    if (!rp) {
-        free(c.base);
-        return SG_ERR_NOMEM;
-    }
-    /* prefix index of a level vector: rank of its first d-2 levels in the
-     * depth-first enumeration; found by a second walk keyed on the vector */
+    if (!rp) return SG_ERR_NOMEM;
+    memset(lv, 0, sizeof(lv));
     for (s = 0; s < L->n; s++)
         for (pos = 0; pos < L->dp[d - 1][s]; pos++) {
-            int a, b, sigma = 0;
-            int64_t pidx = 0;
+            int c, a, b, rem = L->n - 1, sigma = 0;
+            int64_t base = 0, scale = 1;
             sg_eval_shape sh;
+            sg_eval_sub sub;
             sg_layout_idx2l(L, pos, s, lv);
-            /* rank among prefixes: count prefixes that precede lv[0..d-3] */
-            {
-                int rem = L->n - 1;
-                for (k = 0; k < np_dims; k++) {
-                    int l;
-                    for (l = 0; l < lv[k]; l++) pidx += cnt[k + 1][rem - l];
-                    rem -= lv[k];
-                }
+            /* block-layout start of this prefix: the sizes of all prefixes
+             * that precede it in the depth-first walk */
+            for (k = 0; k < np_dims; k++) {
+                int l;
+                for (l = 0; l < lv[k]; l++) base += (sz[k + 1][rem - l] << l) * scale;
+                scale <<= lv[k];
+                rem -= lv[k];
+                sigma += lv[k];
             }
-            for (k = 0; k < np_dims; k++) sigma += lv[k];
+            c = d >= 3 ? lv[d - 3] : 0;
             a = d >= 2 ? lv[d - 2] : 0;
             b = lv[d - 1];
             sg_layout_eval_shape(L, L->n - 1 - sigma, &sh);
+            sg_layout_eval_sub(L, L->n - 1 - sigma - c, &sub);
             rp[r].src = (uint32_t)(L->plidx[s] + (pos << s));
-            rp[r].dst = c.base[pidx] + sh.aoff[a] + (((uint32_t)1 << b) - 1);
-            rp[r].blk = sh.aoff[sh.amax + 1];
-            rp[r].plen = ((uint32_t)1 << sh.rowlen[a]) - 1;
+            rp[r].dst = (uint32_t)base + sh.coff[c] + sub.aoff[a] + (((uint32_t)1 << b) - 1);
+            rp[r].blk = sh.coff[sh.cmax + 1];
+            rp[r].sub = sub.aoff[sub.amax + 1];
+            rp[r].plen = ((uint32_t)1 << sub.rowlen[a]) - 1;
+            rp[r].c = (uint8_t)c;
             rp[r].a = (uint8_t)a;
             rp[r].b = (uint8_t)b;
             rp[r].s = (uint8_t)s;
-            rp[r].pad = 0;
             r++;
         }
-    *prefix_base = c.base;
-    *nprefix = c.np;
     *repack = rp;
     return SG_OK;
 }

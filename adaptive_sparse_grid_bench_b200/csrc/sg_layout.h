@@ -59,37 +59,47 @@ int sg_layout_chains(const sg_layout *L, int k, sg_chain **chains, int64_t *ncha
 
 /*
  * Evaluation layout ("block layout").  The same surpluses, ordered for the
- * evaluation walk: for every prefix level vector p of dims 0..d-3 (depth-
- * first order, level ascending), for every cell I of p (row-major over those
- * dims), one block holding all subspaces (p, a, b) with a = l_{d-2},
- * b = l_{d-1}: rows a = 0..amax, each row 2^a poles (one per cell t_a of dim
- * d-2), each pole the 1-D heap of dim d-1's levels b = 0..rowlen(a)-1 with
- * cell t_b of level b at heap index 2^b - 1 + t_b.  A query point therefore
- * finds every surplus of a block at base + aoff(a) + t_a*plen(a) + 2^b-1 + t_b.
- * For d = 1 the "block" is the single pole of dim 0 (one row, a = 0).
+ * evaluation walk.  Dims 0..d-4 form the prefix; the three innermost dims are
+ * C = d-3, A = d-2, B = d-1 (for d < 3 the missing leading ones are treated
+ * as dims with limit 0).  For every prefix level vector p (depth-first
+ * order, level ascending) and every cell I of p (row-major over the prefix
+ * dims) one block holds all subspaces (p, c, a, b) below the level budget
+ * R = n-1-|p|:
+ *   planes c = 0..cmax, each 2^c sub-blocks (one per cell t_c of dim C);
+ *   a sub-block of budget r = R-c has rows a = 0..amax(r), each 2^a poles
+ *   (one per cell t_a of dim A);
+ *   a pole is the 1-D heap of dim B's levels b = 0..rowlen-1: cell t_b of
+ *   level b sits at 2^b - 1 + t_b.
+ * A query point finds the surplus of (c, a, b) at
+ *   base + coff(c) + t_c * sub(R-c) + aoff(R-c, a) + t_a * plen + 2^b - 1 + t_b.
  */
+typedef struct sg_eval_sub {
+    int amax;                         /* last row: min(r, lim_A)           */
+    int rowlen[SG_MAX_LEVELS];        /* levels of dim B in row a           */
+    uint32_t aoff[SG_MAX_LEVELS + 1]; /* row starts; aoff[amax+1] = size    */
+} sg_eval_sub;
+
 typedef struct sg_eval_shape {
-    int R;         /* level budget n-1-sigma left for the last two dims */
-    int amax;      /* last row: min(R, lim_{d-2}) (0 for d = 1)          */
-    int rowlen[SG_MAX_LEVELS]; /* levels of dim d-1 in row a             */
-    uint32_t aoff[SG_MAX_LEVELS + 1]; /* row starts; aoff[amax+1] = block size */
+    int R, cmax;                      /* budget, last plane min(R, lim_C)   */
+    uint32_t coff[SG_MAX_LEVELS + 1]; /* plane starts; coff[cmax+1] = size  */
 } sg_eval_shape;
 
+void sg_layout_eval_sub(const sg_layout *L, int r, sg_eval_sub *sh);
 void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh);
 
 /* Per-subspace repack descriptor (compact layout -> block layout). */
 typedef struct sg_repack {
     uint32_t src;  /* device offset of the subspace in the group-aligned layout */
-    uint32_t dst;  /* block-layout offset of its element (I=0, t_a=0, t_b=0)    */
-    uint32_t blk;  /* block size: stride between prefix cells I                */
-    uint32_t plen; /* pole length of its row: stride between cells t_a         */
-    uint8_t a, b, s, pad;
+    uint32_t dst;  /* block-layout offset of its element with I = t = 0         */
+    uint32_t blk;  /* block size: stride of the prefix cell I                   */
+    uint32_t sub;  /* sub-block size: stride of t_c                             */
+    uint32_t plen; /* pole length: stride of t_a                                */
+    uint8_t c, a, b, s;
 } sg_repack;
 
-/* Block bases (one per prefix, depth-first order) and the repack table (one
- * entry per subspace).  Both malloc'd. */
-int sg_layout_eval_tables(const sg_layout *L, uint32_t **prefix_base, int64_t *nprefix,
-                          sg_repack **repack);
+/* The repack table (one entry per subspace, malloc'd) and the block sizes
+ * blk3[R] (3-D block) and blk2[r] (sub-block) for every budget. */
+int sg_layout_eval_tables(const sg_layout *L, sg_repack **repack, uint32_t *blk3, uint32_t *blk2);
 
 #ifdef __cplusplus
 }

@@ -27,9 +27,9 @@ struct sg_grid {
     float *d_alpha;   /* Npad floats, group-aligned layout         */
     double *d_work;   /* Npad doubles, FP64 hierarchization (lazy) */
     float *d_blk;        /* N floats: surpluses in the block layout    */
-    uint32_t *d_prefix;  /* block base per prefix                      */
     sg_repack *d_repack; /* per-subspace compact -> block descriptors  */
-    uint32_t blk[SG_MAX_LEVELS]; /* block size per level budget         */
+    uint32_t blk3[SG_MAX_LEVELS]; /* block size per level budget        */
+    uint32_t blk2[SG_MAX_LEVELS]; /* sub-block size per level budget    */
     int eval_dirty;      /* d_blk is stale                              */
     sg_chain *d_chains[SG_MAX_DIMS];
     uint32_t *d_seg[SG_MAX_DIMS];
@@ -109,7 +109,6 @@ static void free_device(sg_grid *g)
     cudaFree(g->d_alpha);
     cudaFree(g->d_work);
     cudaFree(g->d_blk);
-    cudaFree(g->d_prefix);
     cudaFree(g->d_repack);
     for (k = 0; k < SG_MAX_DIMS; k++) {
         cudaFree(g->d_chains[k]);
@@ -246,9 +245,7 @@ static void leave(sg_grid *g, int prev)
 static int materialize(sg_grid *g)
 {
     const sg_layout *L = &g->L;
-    uint32_t *prefix = NULL;
     sg_repack *rp = NULL;
-    int64_t nprefix = 0;
     int k, r;
     if (g->dev >= 0) return SG_OK;
     CU(cudaGetDevice(&g->dev), "cudaGetDevice");
@@ -256,24 +253,15 @@ static int materialize(sg_grid *g)
     CU(cudaMemset(g->d_alpha, 0, (size_t)L->Npad * 4), "cudaMemset");
     if ((r = dev_alloc(g, (void **)&g->d_err, 16, "error flag")) != SG_OK) goto bad;
     CU(cudaMemset(g->d_err, 0, 16), "cudaMemset");
-    if ((r = sg_layout_eval_tables(L, &prefix, &nprefix, &rp)) != SG_OK) {
+    if ((r = sg_layout_eval_tables(L, &rp, g->blk3, g->blk2)) != SG_OK) {
         fail(r, "building the evaluation layout tables");
         goto bad;
     }
-    for (k = 0; k < L->n; k++) {
-        sg_eval_shape sh;
-        sg_layout_eval_shape(L, k, &sh);
-        g->blk[k] = sh.aoff[sh.amax + 1];
-    }
     if ((r = dev_alloc(g, (void **)&g->d_blk, L->N * 4, "block layout")) != SG_OK) goto bad;
-    if ((r = dev_alloc(g, (void **)&g->d_prefix, nprefix * 4, "block bases")) != SG_OK) goto bad;
     if ((r = dev_alloc(g, (void **)&g->d_repack, L->S * (int64_t)sizeof(sg_repack), "repack table")) != SG_OK)
         goto bad;
-    CU(cudaMemcpy(g->d_prefix, prefix, (size_t)nprefix * 4, cudaMemcpyHostToDevice), "cudaMemcpy");
     CU(cudaMemcpy(g->d_repack, rp, (size_t)L->S * sizeof(sg_repack), cudaMemcpyHostToDevice), "cudaMemcpy");
-    free(prefix);
     free(rp);
-    prefix = NULL;
     rp = NULL;
     g->eval_dirty = 1;
     for (k = 0; k < L->d; k++) {
@@ -316,7 +304,6 @@ static int materialize(sg_grid *g)
     }
     return SG_OK;
 bad:
-    free(prefix);
     free(rp);
     free_device(g);
     memset(g->d_chains, 0, sizeof(g->d_chains));
@@ -324,7 +311,6 @@ bad:
     g->d_alpha = NULL;
     g->d_work = NULL;
     g->d_blk = NULL;
-    g->d_prefix = NULL;
     g->d_repack = NULL;
     g->d_err = NULL;
     g->d_scratch = g->d_io = NULL;
@@ -527,7 +513,7 @@ static int ensure(sg_grid *g, void **buf, int64_t *have, int64_t need, const cha
 static int eval_ppt(const sg_grid *g)
 {
     if (g->opt[SG_OPT_EVAL_PPT] == 1 || g->opt[SG_OPT_EVAL_PPT] == 2) return (int)g->opt[SG_OPT_EVAL_PPT];
-    return 1;
+    return 2;
 }
 
 static int evaluate_on(sg_grid *g, const float *coords, float *out, int64_t m, cudaStream_t st)
@@ -540,11 +526,13 @@ static int evaluate_on(sg_grid *g, const float *coords, float *out, int64_t m, c
         g->eval_dirty = 0;
     }
     p.alpha = g->d_blk;
-    p.prefix_base = g->d_prefix;
     p.d = g->L.d;
     p.n = g->L.n;
     for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < g->L.d ? g->L.lim[k] : 0;
-    for (k = 0; k < SG_MAX_LEVELS; k++) p.blk[k] = g->blk[k];
+    for (k = 0; k < SG_MAX_LEVELS; k++) {
+        p.blk3[k] = g->blk3[k];
+        p.blk2[k] = g->blk2[k];
+    }
     p.ppt = eval_ppt(g);
     if (g->opt[SG_OPT_EVAL_SORT] && m > 1) {
         const int64_t sort_b = (sgk_sort_scratch_bytes(m, p.d) + 255) & ~(int64_t)255;
