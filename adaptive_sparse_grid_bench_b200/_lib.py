@@ -74,6 +74,7 @@ SIGNATURES = {
     "sg_get_option": (_i, [_p, _i, _pi64]),
     "sg_device_bytes": (_i, [_p, _pi64]),
     "sg_timings": (_i, [_p, _p]),
+    "sg_kernel_launches": (_i, [_pi64]),
     "sg_sample_function": (_i, [_p, _i, _p, _i, _p]),
     "sg_last_error": (C.c_char_p, []),
     "sg_version": (C.c_char_p, []),
@@ -103,6 +104,13 @@ def lib() -> C.CDLL:
             f.argtypes = args
         _lib = L
     return _lib
+
+
+def kernel_launches() -> int:
+    """Kernels launched by libsgb200.so so far in this process."""
+    v = C.c_int64()
+    check(lib().sg_kernel_launches(C.byref(v)))
+    return v.value
 
 
 class SgError(RuntimeError):

@@ -165,6 +165,7 @@ int sgk_idx2gp(const sg_layout *L, const int64_t *index, int *levels, int *indic
     if (g > 148 * 16) g = 148 * 16;
     k_idx2gp<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(make_tables(L), index, levels, indices,
                                                            count);
+    sgk_count(1);
     return cudaGetLastError();
 }
 
@@ -176,6 +177,7 @@ int sgk_gp2idx(const sg_layout *L, const int *levels, const int *indices, int64_
     if (g > 148 * 16) g = 148 * 16;
     k_gp2idx<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(make_tables(L), levels, indices, index,
                                                            count);
+    sgk_count(1);
     return cudaGetLastError();
 }
 
@@ -189,6 +191,7 @@ int sgk_sample(const sg_layout *L, int fn, const double *params, int nparams, fl
     int64_t g = (L->Npad + 255) / 256;
     if (g > 148 * 32) g = 148 * 32;
     k_sample<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(make_tables(L), F, alpha, L->Npad);
+    sgk_count(1);
     return cudaGetLastError();
 }
 

@@ -405,6 +405,7 @@ int launch_eval(const EvalArgs &A, void *stream)
     const int64_t blocks = (A.num_evals + per_block - 1) / per_block;
     if (blocks > 0x7fffffff) return cudaErrorInvalidValue;
     k_evaluate<D, P><<<(unsigned)blocks, kThreads, 0, (cudaStream_t)stream>>>(A);
+    sgk_count(1);
     return cudaGetLastError();
 }
 

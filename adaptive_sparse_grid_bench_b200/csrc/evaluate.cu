@@ -166,16 +166,21 @@ int scan_exclusive(uint32_t *v, int64_t m, uint32_t *tmp, cudaStream_t st)
     const int64_t b1 = (m + per - 1) / per;
     uint32_t *t1 = tmp;
     k_scan_blocks<<<(unsigned)b1, kThreads, 0, st>>>(v, m, t1);
+    sgk_count(1);
     if (b1 > 1) {
         const int64_t b2 = (b1 + per - 1) / per;
         uint32_t *t2 = tmp + b1;
         k_scan_blocks<<<(unsigned)b2, kThreads, 0, st>>>(t1, b1, t2);
+        sgk_count(1);
         if (b2 > 1) {
             if (b2 > per) return cudaErrorInvalidValue;
             k_scan_blocks<<<1, kThreads, 0, st>>>(t2, b2, nullptr);
+            sgk_count(1);
             k_scan_add<<<(unsigned)b2, kThreads, 0, st>>>(t1, b1, t2);
+            sgk_count(1);
         }
         k_scan_add<<<(unsigned)b1, kThreads, 0, st>>>(v, m, t1);
+        sgk_count(1);
     }
     return cudaGetLastError();
 }
@@ -220,6 +225,7 @@ int sgk_repack(const float *src, float *dst, const sg_repack *rp, int64_t nsub, 
     if (nsub <= 0) return cudaSuccess;
     int64_t g = nsub < 148 * 64 ? nsub : 148 * 64;
     k_repack<<<(unsigned)g, 128, 0, (cudaStream_t)stream>>>(src, dst, rp, nsub);
+    sgk_count(1);
     return cudaGetLastError();
 }
 
@@ -245,9 +251,11 @@ int sgk_sort_points(const float *coords, int64_t n, int d, void *scratch, float 
     int64_t g = (n + 255) / 256;
     if (g > 148 * 16) g = 148 * 16;
     k_sort_keys<<<(unsigned)g, 256, 0, st>>>(coords, n, d, kb, keys, hist);
+    sgk_count(1);
     int r = scan_exclusive(hist, bins, tmp, st);
     if (r != cudaSuccess) return r;
     k_sort_scatter<<<(unsigned)g, 256, 0, st>>>(coords, n, d, keys, hist, sorted, perm);
+    sgk_count(1);
     return cudaGetLastError();
 }
 

@@ -305,6 +305,7 @@ __global__ void k_narrow(const double *__restrict__ s, float *__restrict__ d, in
 }
 
 int g_num_sms = 0;
+long long g_launches = 0;
 
 template <typename T>
 int launch_chains(T *a, const sg_sweep_tables *t, int *err, void *stream)
@@ -326,6 +327,7 @@ int launch_chains(T *a, const sg_sweep_tables *t, int *err, void *stream)
     if (grid > t->nchains) grid = t->nchains;
     k_sweep_chains<T><<<(unsigned)grid, kThreads, (size_t)smem, (cudaStream_t)stream>>>(
         a, t->chains, t->seg, (int)t->nchains, capi, err);
+    sgk_count(1);
     return cudaGetLastError();
 }
 
@@ -338,6 +340,7 @@ int launch_gather(T *a, const sg_sweep_tables *t, void *stream)
     for (int j = t->lmax_max; j >= 1; --j) {
         k_sweep_gather<T><<<(unsigned)grid, kThreads, 0, (cudaStream_t)stream>>>(
             a, t->chains, t->seg, (int)t->nchains, j);
+        sgk_count(1);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -347,6 +350,9 @@ int launch_gather(T *a, const sg_sweep_tables *t, void *stream)
 } // namespace
 
 extern "C" {
+
+void sgk_count(int launches) { __atomic_fetch_add(&g_launches, (long long)launches, __ATOMIC_RELAXED); }
+int64_t sgk_launches(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 int sgk_num_sms(void)
 {
@@ -389,6 +395,7 @@ int sgk_widen(const float *src, double *dst, int64_t n, void *stream)
     int64_t g = (n + 255) / 256;
     if (g > 148 * 32) g = 148 * 32;
     k_widen<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(src, dst, n);
+    sgk_count(1);
     return cudaGetLastError();
 }
 
@@ -398,6 +405,7 @@ int sgk_narrow(const double *src, float *dst, int64_t n, void *stream)
     int64_t g = (n + 255) / 256;
     if (g > 148 * 32) g = 148 * 32;
     k_narrow<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(src, dst, n);
+    sgk_count(1);
     return cudaGetLastError();
 }
 

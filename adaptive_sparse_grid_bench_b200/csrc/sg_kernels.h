@@ -75,6 +75,10 @@ int sgk_sample(const sg_layout *L, int fn, const double *params, int nparams, fl
 
 int sgk_num_sms(void);
 
+/* Process-wide count of kernels this library has launched. */
+void sgk_count(int launches);
+int64_t sgk_launches(void);
+
 #ifdef __cplusplus
 }
 #endif

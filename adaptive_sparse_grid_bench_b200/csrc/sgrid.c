@@ -680,6 +680,13 @@ SG_API int sg_get_option(const sg_grid *g, int option, int64_t *value)
     return SG_OK;
 }
 
+SG_API int sg_kernel_launches(int64_t *count)
+{
+    if (!count) return fail(SG_ERR_ARG, "sg_kernel_launches: NULL argument");
+    *count = sgk_launches();
+    return SG_OK;
+}
+
 SG_API int sg_device_bytes(const sg_grid *g, int64_t *bytes)
 {
     if (!g || !bytes) return fail(SG_ERR_ARG, "sg_device_bytes: NULL argument");

@@ -219,8 +219,10 @@ def run_b200(args, rank: int, world: int, local_rank: int):
     g.sync(stream)
     barrier()
     t_hier, t_eval, t_sort = [], [], []
+    from adaptive_sparse_grid_bench_b200._lib import kernel_launches
     with Clocks(local_rank) as clk:
         barrier()
+        launches0 = kernel_launches()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -232,6 +234,7 @@ def run_b200(args, rank: int, world: int, local_rank: int):
             t_eval.append(t["evaluate"])
         e1.record(stream)
         barrier()
+        launches = kernel_launches() - launches0
     g.sync(stream)
     ms = e0.elapsed_time(e1)
     ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -303,14 +306,9 @@ def run_b200(args, rank: int, world: int, local_rank: int):
                      "traffic": None, "kernel": "k_evaluate", "peak_source": peak_src,
                      "bytes": "4*(S+d+1) per query point (cache-served surplus reads counted)"},
         "e2e": e2e,
-        "gpu_launches": None,
+        "gpu_launches": int(launches),
         "clocks": clocks,
     }
-    # launches per step: set_values (n D2D copies are not kernels) + d sweeps
-    # (+2 conversions in fp64) + sort (memset is not a kernel: keys, 1-3 scan
-    # levels, scatter) + evaluate
-    sweeps = D + (2 if args.precision == "fp64" else 0)
-    line["gpu_launches"] = args.steps * (sweeps + 1 + 2 + 3 + 1)
     if world == 1 and not args.no_cpu_baseline:
         vals = vals_d.cpu().numpy()
         cpu_v, info = reference_cpu(vals, X, args.cpu_seconds)

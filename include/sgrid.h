@@ -143,6 +143,9 @@ int sg_get_option(const sg_grid *grid, int option, int64_t *value);
 /* Device time of each phase of the most recent calls made with
  * SG_OPT_PROFILE on (waits for them); ms[SG_NUM_PHASES], -1 if not run. */
 int sg_timings(sg_grid *grid, double *ms);
+/* Number of kernels this library has launched in this process (all
+ * handles); a difference of two readings counts the launches in between. */
+int sg_kernel_launches(int64_t *count);
 /* Bytes of device memory the handle holds (grid, tables and scratch). */
 int sg_device_bytes(const sg_grid *grid, int64_t *bytes);
 /* Text of the last error raised on the calling thread ("" if none). */
