@@ -41,6 +41,8 @@ SG_FN_QUAD = 4
 
 SG_MAX_DIMS = 20
 SG_MAX_LEVELS = 16
+SG_NOALLOC_MAX_POINTS = 1 << 18
+SG_NOALLOC_SCRATCH_BYTES = 24 << 20
 
 _i = C.c_int
 _i64 = C.c_int64
@@ -67,6 +69,7 @@ SIGNATURES = {
     "sg_get_values_device": (_i, [_p, _p, _p]),
     "sg_hierarchize_async": (_i, [_p, _p]),
     "sg_evaluate_device": (_i, [_p, _p, _p, _i64, _p]),
+    "sg_evaluate_device_noalloc": (_i, [_p, _p, _p, _i64, _p]),
     "sg_sync": (_i, [_p, _p]),
     "sg_idx2gp_device": (_i, [_p, _p, _p, _p, _i64, _p]),
     "sg_gp2idx_device": (_i, [_p, _p, _p, _p, _i64, _p]),

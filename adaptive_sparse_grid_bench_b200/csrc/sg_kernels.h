@@ -75,6 +75,10 @@ int sgk_sample(const sg_layout *L, int fn, const double *params, int nparams, fl
 
 int sgk_num_sms(void);
 
+/* Device address and size of the fixed no-allocation scratch array on the
+ * current device (looked up on the first call per device). */
+int sgk_noalloc_scratch(void **ptr, int64_t *bytes);
+
 /* Process-wide count of kernels this library has launched. */
 void sgk_count(int launches);
 int64_t sgk_launches(void);

@@ -571,6 +571,63 @@ SG_API int sg_evaluate_device(sg_grid *g, const float *coords, float *out, int64
     return r;
 }
 
+/* The no-allocation evaluation: as evaluate_on with sorting, but every
+ * scratch region is carved from the library's fixed device array and no
+ * device memory, event or other resource is created. */
+SG_API int sg_evaluate_device_noalloc(sg_grid *g, const float *coords, float *out, int64_t m, void *stream)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    sg_eval_plan p;
+    int prev, r = SG_OK, e, k;
+    void *scratch = NULL;
+    int64_t have = 0, sort_b, coords_b;
+    if (!g || m < 0 || (m > 0 && (!coords || !out))) return fail(SG_ERR_ARG, "sg_evaluate_device_noalloc: bad argument");
+    if (!g->has_values || g->dev < 0)
+        return fail(SG_ERR_STATE, "sg_evaluate_device_noalloc: the grid has no device state yet (set values first)");
+    if (m > SG_NOALLOC_MAX_POINTS)
+        return fail(SG_ERR_RANGE, "sg_evaluate_device_noalloc: %lld points exceed SG_NOALLOC_MAX_POINTS (%d)",
+                    (long long)m, SG_NOALLOC_MAX_POINTS);
+    if (m == 0) return SG_OK;
+    sort_b = (sgk_sort_scratch_bytes(m, g->L.d) + 255) & ~(int64_t)255;
+    coords_b = (m * g->L.d * 4 + 255) & ~(int64_t)255;
+    if ((r = enter(g, &prev)) != SG_OK) return r;
+    if ((e = sgk_noalloc_scratch(&scratch, &have)) != cudaSuccess) {
+        r = cuda_fail((cudaError_t)e, "sg_evaluate_device_noalloc: scratch address");
+    } else if (sort_b + coords_b + m * 4 > have) {
+        r = fail(SG_ERR_RANGE, "sg_evaluate_device_noalloc: %lld points in %d dims need more than the %lld-byte scratch",
+                 (long long)m, g->L.d, (long long)have);
+    } else {
+        char *base = (char *)scratch;
+        float *sorted = (float *)(base + sort_b);
+        int32_t *perm = (int32_t *)(base + sort_b + coords_b);
+        if (g->eval_dirty) {
+            if ((e = sgk_repack(g->d_alpha, g->d_blk, g->d_repack, g->L.S, st)) != cudaSuccess)
+                r = cuda_fail((cudaError_t)e, "repacking surpluses");
+            else
+                g->eval_dirty = 0;
+        }
+        if (r == SG_OK) {
+            p.alpha = g->d_blk;
+            p.d = g->L.d;
+            p.n = g->L.n;
+            for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < g->L.d ? g->L.lim[k] : 0;
+            for (k = 0; k < SG_MAX_LEVELS; k++) {
+                p.blk3[k] = g->blk3[k];
+                p.blk2[k] = g->blk2[k];
+            }
+            p.ppt = eval_ppt(g);
+            /* the histogram is cleared inside the sort, so nothing left in
+             * the shared array by an earlier call is read */
+            if ((e = sgk_sort_points(coords, m, p.d, base, sorted, perm, st)) != cudaSuccess)
+                r = cuda_fail((cudaError_t)e, "sorting query points");
+            else if ((e = sgk_evaluate(&p, sorted, perm, out, m, st)) != cudaSuccess)
+                r = cuda_fail((cudaError_t)e, "evaluate");
+        }
+    }
+    leave(g, prev);
+    return r;
+}
+
 SG_API int sg_evaluate(sg_grid *g, const float *coords, float *out, int64_t m)
 {
     int prev, r;

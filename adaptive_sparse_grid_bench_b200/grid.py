@@ -194,6 +194,14 @@ class Grid:
         check(L.lib().sg_sample_function(self._h, int(fn), _ptr(p) if p.size else None, int(p.size),
                                          _stream_handle(stream)))
 
+    def evaluate_device_noalloc(self, coords, out, num_evals: int | None = None, stream=None) -> None:
+        """sg_evaluate_device_noalloc: the same evaluation without any device
+        allocation (fixed scratch; at most SG_NOALLOC_MAX_POINTS points)."""
+        if num_evals is None:
+            num_evals = int(coords.shape[0])
+        check(L.lib().sg_evaluate_device_noalloc(self._h, self._dptr(coords), self._dptr(out), int(num_evals),
+                                                 _stream_handle(stream)))
+
     def sync(self, stream=None) -> None:
         check(L.lib().sg_sync(self._h, _stream_handle(stream)))
 

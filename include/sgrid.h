@@ -112,6 +112,28 @@ int sg_get_values_device(sg_grid *grid, float *values, void *stream);
 int sg_hierarchize_async(sg_grid *grid, void *stream);
 int sg_evaluate_device(sg_grid *grid, const float *coord_mat, float *out,
                        int64_t num_evals, void *stream);
+/* Evaluation that allocates no memory, for callers that cannot call
+ * cudaMalloc at evaluation time: serving loops whose device memory is
+ * reserved up front by their own pool, latency-bound request paths that
+ * cannot afford cudaMalloc's device synchronisation, and hosts that forbid
+ * plugins from allocating device memory.  No counterpart in the reference.
+ * Same meaning and result as sg_evaluate_device, but the point-sorting
+ * scratch is a fixed array of SG_NOALLOC_SCRATCH_BYTES in this library that
+ * every GPU loading the library holds until the process exits.  Limits: the
+ * handle's device state must already exist (created by an earlier
+ * sg_set_values*, sg_sample_function or sg_hierarchize* call on this
+ * device, else SG_ERR_STATE) and num_evals <= SG_NOALLOC_MAX_POINTS (else
+ * SG_ERR_RANGE).  The first call on a device looks up the array's device
+ * address, which makes the CUDA runtime place the array on that device;
+ * make that first call before capturing work on the stream.  All
+ * calls share the one array: calls whose work overlaps on the GPU (other
+ * streams, other handles, other host threads) race and must be serialised
+ * by the caller. */
+#define SG_NOALLOC_MAX_POINTS (1 << 18)
+#define SG_NOALLOC_SCRATCH_BYTES (24 << 20)
+int sg_evaluate_device_noalloc(sg_grid *grid, const float *coord_mat, float *out,
+                               int64_t num_evals, void *stream);
+
 /* Waits for `stream` and reports any device-side error flag of the handle. */
 int sg_sync(sg_grid *grid, void *stream);
 
