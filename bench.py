@@ -192,6 +192,7 @@ def run_b200(args, rank: int, world: int, local_rank: int):
     import torch.distributed as dist
     from adaptive_sparse_grid_bench_b200 import Grid
     from adaptive_sparse_grid_bench_b200._lib import SG_OPT_PROFILE
+    from adaptive_sparse_grid_bench_b200.sharding import max_over_ranks
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -237,10 +238,7 @@ def run_b200(args, rank: int, world: int, local_rank: int):
         launches = kernel_launches() - launches0
     g.sync(stream)
     ms = e0.elapsed_time(e1)
-    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
-    ms_max = float(ms_t.item())
+    ms_max = max_over_ranks(ms, dev) if world > 1 else ms
     value = world * m * args.steps / (ms_max / 1e3)
 
     # end-to-end through the host-buffer C ABI, copies inside the timed region
@@ -269,10 +267,10 @@ def run_b200(args, rank: int, world: int, local_rank: int):
             step_e2e()
         s1.record()
         barrier()
-        e_ms = torch.tensor([s0.elapsed_time(s1)], dtype=torch.float64, device=dev)
+        e_ms = s0.elapsed_time(s1)
         if world > 1:
-            dist.all_reduce(e_ms, op=dist.ReduceOp.MAX)
-        e2e = {"value": world * m * args.steps / (float(e_ms.item()) / 1e3), "unit": "evals/s",
+            e_ms = max_over_ranks(e_ms, dev)
+        e2e = {"value": world * m * args.steps / (e_ms / 1e3), "unit": "evals/s",
                "h2d_bytes_per_step": int(g.num_points * 4 + m * D * 4), "d2h_bytes_per_step": int(m * 4)}
         if not np.array_equal(oh, out_d.cpu().numpy()):
             raise RuntimeError("host-buffer and device-pointer evaluations differ")
