@@ -29,6 +29,7 @@
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kMaxStages = 2;
 constexpr long long kWaitCycles = 4000000000LL; /* ~2 s at 1.9 GHz */
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -151,24 +152,96 @@ __device__ __forceinline__ T chain_point(const T *buf, int sigma, int lo, int j,
     return upd(buf[seg_soff<A>(sigma, j) + p], lft, rgt);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_sweep_chains(T *__restrict__ a,
+/* Shared-memory index of the 1-D node at position m / 2^j of pole (hi, lw):
+ * m odd-multiple of 2^tz is the point of level j-1-tz, index m >> (tz+1).
+ * Valid for 0 < m < 2^j (the ends of the pole are the domain boundary). */
+__device__ __forceinline__ int node_index(int sigma, int lo, int j, int hi, int lw, int m)
+{
+    const int tz = __ffs(m) - 1;
+    const int pl = j - 1 - tz;
+    return seg_soff<4>(sigma, pl) + ((((hi << pl) | (m >> (tz + 1))) << lo) | lw);
+}
+
+__device__ __forceinline__ float node_value(const float *buf, int sigma, int lo, int j, int hi, int lw, int m)
+{
+    return (m == 0 || m == (1 << j)) ? 0.0f : buf[node_index(sigma, lo, j, hi, lw, m)];
+}
+
+/* Four consecutive updated points p..p+3 of segment j (FP32, sigma >= 2, so
+ * p is a multiple of 4 and the group lies in one segment).  Each output is
+ * upd(self, V(i_k), V(i_k + 1)) with V the pre-sweep value at the point's
+ * left/right 1-D neighbour, exactly as chain_point computes it; the groups
+ * only share the loads:
+ *   lo >= 2: the 4 points differ in the low dims only -> 4-wide loads;
+ *   lo == 1: two i_k values x two low cells -> 2-wide loads;
+ *   lo == 0: four consecutive i_k of one pole (j >= 2) -> 5 neighbours. */
+__device__ __forceinline__ float4 chain_group4(const float *buf, int sigma, int lo, int j, int p)
+{
+    const float4 self = *reinterpret_cast<const float4 *>(buf + seg_soff<4>(sigma, j) + p);
+    float4 o;
+    if (lo >= 2) {
+        const int ik = (p >> lo) & ((1 << j) - 1);
+        const int hi = p >> (lo + j);
+        const int lw = p & ((1 << lo) - 1);
+        float4 L = make_float4(0.f, 0.f, 0.f, 0.f), R = L;
+        if (ik != 0) L = *reinterpret_cast<const float4 *>(buf + node_index(sigma, lo, j, hi, lw, ik));
+        if (ik + 1 != (1 << j)) R = *reinterpret_cast<const float4 *>(buf + node_index(sigma, lo, j, hi, lw, ik + 1));
+        o.x = upd(self.x, L.x, R.x);
+        o.y = upd(self.y, L.y, R.y);
+        o.z = upd(self.z, L.z, R.z);
+        o.w = upd(self.w, L.w, R.w);
+    } else if (lo == 1) {
+        const int ik = (p >> 1) & ((1 << j) - 1); /* even */
+        const int hi = p >> (1 + j);
+        float2 v0 = make_float2(0.f, 0.f), v2 = v0;
+        if (ik != 0) v0 = *reinterpret_cast<const float2 *>(buf + node_index(sigma, 1, j, hi, 0, ik));
+        const float2 v1 = *reinterpret_cast<const float2 *>(buf + node_index(sigma, 1, j, hi, 0, ik + 1));
+        if (ik + 2 != (1 << j)) v2 = *reinterpret_cast<const float2 *>(buf + node_index(sigma, 1, j, hi, 0, ik + 2));
+        o.x = upd(self.x, v0.x, v1.x);
+        o.y = upd(self.y, v0.y, v1.y);
+        o.z = upd(self.z, v1.x, v2.x);
+        o.w = upd(self.w, v1.y, v2.y);
+    } else if (j >= 2) {
+        const int ik = p & ((1 << j) - 1); /* multiple of 4 */
+        const int hi = p >> j;
+        const float2 odd = *reinterpret_cast<const float2 *>(buf + seg_soff<4>(sigma, j - 1) + (hi << (j - 1)) + (ik >> 1));
+        const float mid = buf[seg_soff<4>(sigma, j - 2) + (hi << (j - 2)) + (ik >> 2)];
+        const float v0 = node_value(buf, sigma, 0, j, hi, 0, ik);
+        const float v4 = node_value(buf, sigma, 0, j, hi, 0, ik + 4);
+        o.x = upd(self.x, v0, odd.x);
+        o.y = upd(self.y, odd.x, mid);
+        o.z = upd(self.z, mid, odd.y);
+        o.w = upd(self.w, odd.y, v4);
+    } else {
+        o.x = chain_point<float, 4>(buf, sigma, lo, j, p);
+        o.y = chain_point<float, 4>(buf, sigma, lo, j, p + 1);
+        o.z = chain_point<float, 4>(buf, sigma, lo, j, p + 2);
+        o.w = chain_point<float, 4>(buf, sigma, lo, j, p + 3);
+    }
+    return o;
+}
+
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) k_sweep_chains(T *__restrict__ a,
                                                           const sg_chain *__restrict__ chains,
                                                           const uint32_t *__restrict__ seg,
-                                                          int nch, int cap, int *__restrict__ err)
+                                                          int nch, int cap, int nst, int *__restrict__ err)
 {
     constexpr int A = 16 / sizeof(T); /* elements per 16 bytes */
     using V = typename Vec<T>::type;
     constexpr int W = Vec<T>::W;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[kMaxStages];
     __shared__ int s_abort;
-    T *stage[2] = {reinterpret_cast<T *>(smem_raw), reinterpret_cast<T *>(smem_raw) + cap};
+    T *const stage0 = reinterpret_cast<T *>(smem_raw);
     const int G = gridDim.x;
     const int tid = threadIdx.x;
 
+    /* chain c goes to stage b; the stage's barrier completes when all its
+     * bulk copies have landed */
     auto issue = [&](int c, int b) {
         const sg_chain ch = chains[c];
+        T *dst = stage0 + (size_t)b * cap;
         uint32_t bytes = 0;
         for (int j = 0; j <= ch.lmax; ++j) {
             const uint32_t sz = (uint32_t)sizeof(T) << (ch.sigma + j);
@@ -178,30 +251,27 @@ __global__ void __launch_bounds__(kThreads) k_sweep_chains(T *__restrict__ a,
         mbar_arrive_expect_tx(&bar[b], bytes);
         for (int j = 0; j <= ch.lmax; ++j) {
             const uint32_t sz = (uint32_t)sizeof(T) << (ch.sigma + j);
-            if (sz >= 16)
-                bulk_load(stage[b] + seg_soff<A>(ch.sigma, j), a + seg[ch.seg + j], sz, &bar[b]);
+            if (sz >= 16) bulk_load(dst + seg_soff<A>(ch.sigma, j), a + seg[ch.seg + j], sz, &bar[b]);
         }
     };
 
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int b = 0; b < nst; ++b) mbar_init(&bar[b], 1);
         s_abort = 0;
         fence_mbar_init();
     }
     __syncthreads();
-    if (tid == 0) {
-        if (blockIdx.x < nch) issue(blockIdx.x, 0);
-        if (blockIdx.x + G < nch) issue(blockIdx.x + G, 1);
-    }
+    if (tid == 0)
+        for (int b = 0; b < nst; ++b)
+            if (blockIdx.x + b * G < nch) issue(blockIdx.x + b * G, b);
 
     int it = 0, abort_it = -1;
     for (int c = blockIdx.x; c < nch; c += G, ++it) {
-        const int b = it & 1;
-        const uint32_t parity = (it >> 1) & 1;
+        const int b = it % nst;
+        const uint32_t parity = (it / nst) & 1;
         const sg_chain ch = chains[c];
         const int sigma = ch.sigma, lo = ch.lo, lmax = ch.lmax;
-        T *buf = stage[b];
+        T *buf = stage0 + (size_t)b * cap;
         if (!mbar_wait(&bar[b], parity)) {
             atomicExch(err, 1);
             s_abort = 1;
@@ -222,37 +292,34 @@ __global__ void __launch_bounds__(kThreads) k_sweep_chains(T *__restrict__ a,
          * q = 2^sigma (2^j - 2) */
         const int U = (((2 << lmax) - 2) << sigma);
         if ((1 << sigma) >= W) {
-            for (int v = tid; v < U / W; v += kThreads) {
+            for (int v = tid; v < U / W; v += NT) {
                 const int q = v * W;
                 const int j = 31 - __clz((q >> sigma) + 2);
                 const int p = q - (((1 << j) - 2) << sigma);
-                T r[W];
-#pragma unroll
-                for (int e = 0; e < W; ++e) r[e] = chain_point<T, A>(buf, sigma, lo, j, p + e);
                 V out;
                 if constexpr (W == 4) {
-                    out = make_float4(r[0], r[1], r[2], r[3]);
+                    out = chain_group4(buf, sigma, lo, j, p);
                 } else {
-                    out = make_double2(r[0], r[1]);
+                    out = make_double2(chain_point<T, A>(buf, sigma, lo, j, p),
+                                       chain_point<T, A>(buf, sigma, lo, j, p + 1));
                 }
                 *reinterpret_cast<V *>(a + seg[ch.seg + j] + p) = out;
             }
         } else {
-            for (int q = tid; q < U; q += kThreads) {
+            for (int q = tid; q < U; q += NT) {
                 const int j = 31 - __clz((q >> sigma) + 2);
                 const int p = q - (((1 << j) - 2) << sigma);
                 a[seg[ch.seg + j] + p] = chain_point<T, A>(buf, sigma, lo, j, p);
             }
         }
         __syncthreads(); /* every read of stage b is done */
-        if (tid == 0 && c + 2 * G < nch) issue(c + 2 * G, b);
+        if (tid == 0 && c + nst * G < nch) issue(c + nst * G, b);
     }
     if (abort_it >= 0 && tid == 0) {
-        /* let the copies still in flight land before the CTA exits: the stage
-         * that timed out and, if it was issued, the next one (bounded) */
-        (void)mbar_wait(&bar[abort_it & 1], (abort_it >> 1) & 1);
-        if (blockIdx.x + (abort_it + 1) * G < nch)
-            (void)mbar_wait(&bar[(abort_it + 1) & 1], ((abort_it + 1) >> 1) & 1);
+        /* let the copies still in flight land before the CTA exits: every
+         * stage issued for iterations abort_it .. abort_it+nst-1 (bounded) */
+        for (int q = abort_it; q < abort_it + nst; ++q)
+            if (blockIdx.x + q * G < nch) (void)mbar_wait(&bar[q % nst], (q / nst) & 1);
     }
 }
 
@@ -307,28 +374,41 @@ __global__ void k_narrow(const double *__restrict__ s, float *__restrict__ d, in
 int g_num_sms = 0;
 long long g_launches = 0;
 
+template <typename T, int NT>
+int launch_chains_nt(T *a, const sg_sweep_tables *t, int64_t cap, int *err, void *stream)
+{
+    const int64_t stage_bytes = (cap * (int64_t)sizeof(T) + 127) / 128 * 128;
+    /* as many stages (2..kMaxStages) as fit in 96 KB */
+    int nst = (int)((96 * 1024) / stage_bytes);
+    nst = nst < 2 ? 2 : (nst > kMaxStages ? kMaxStages : nst);
+    const int64_t smem = nst * stage_bytes;
+    const int capi = (int)(stage_bytes / (int64_t)sizeof(T));
+    cudaError_t e = cudaFuncSetAttribute(k_sweep_chains<T, NT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chains<T, NT>, NT, (size_t)smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)sgk_num_sms() * per_sm;
+    if (grid > t->nchains) grid = t->nchains;
+    k_sweep_chains<T, NT><<<(unsigned)grid, NT, (size_t)smem, (cudaStream_t)stream>>>(
+        a, t->chains, t->seg, (int)t->nchains, capi, nst, err);
+    sgk_count(1);
+    return cudaGetLastError();
+}
+
+/* CTA size follows the chain size: up to 12 elements (three 16-byte groups)
+ * per thread, between 128 and 512 threads. */
 template <typename T>
 int launch_chains(T *a, const sg_sweep_tables *t, int *err, void *stream)
 {
     if (t->nchains == 0) return cudaSuccess;
     const int64_t cap = sizeof(T) == 4 ? t->cap32 : t->cap64;
-    const int64_t smem = sgk_chain_smem_bytes(cap, (int)sizeof(T));
-    if (smem < 0) return cudaErrorInvalidValue;
-    const int capi = (int)((smem / 2) / (int64_t)sizeof(T));
-    cudaError_t e = cudaFuncSetAttribute(k_sweep_chains<T>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_chains<T>, kThreads,
-                                                      (size_t)smem);
-    if (e != cudaSuccess) return e;
-    if (per_sm < 1) per_sm = 1;
-    int64_t grid = (int64_t)sgk_num_sms() * per_sm;
-    if (grid > t->nchains) grid = t->nchains;
-    k_sweep_chains<T><<<(unsigned)grid, kThreads, (size_t)smem, (cudaStream_t)stream>>>(
-        a, t->chains, t->seg, (int)t->nchains, capi, err);
-    sgk_count(1);
-    return cudaGetLastError();
+    if (sgk_chain_smem_bytes(cap, (int)sizeof(T)) < 0) return cudaErrorInvalidValue;
+    if (cap <= 128 * 12) return launch_chains_nt<T, 128>(a, t, cap, err, stream);
+    if (cap <= 256 * 12) return launch_chains_nt<T, 256>(a, t, cap, err, stream);
+    return launch_chains_nt<T, 512>(a, t, cap, err, stream);
 }
 
 template <typename T>
