@@ -7,6 +7,7 @@ only binds it (`Grid`) and generates seeded inputs (`inputs`).
 from ._lib import (SG_HIER_FP32, SG_HIER_FP64, SG_OPT_EVAL_BLOCKS, SG_OPT_EVAL_PPT,  # noqa: F401
                    SG_OPT_EVAL_SORT, SG_OPT_HIER_KERNEL, SG_OPT_HIER_PRECISION, SG_OPT_PROFILE, SgError,
                    header_functions, lib)
+from .batch import Batch  # noqa: F401
 from .grid import Grid  # noqa: F401
 
-__all__ = ["Grid", "SgError", "lib", "header_functions"]
+__all__ = ["Grid", "Batch", "SgError", "lib", "header_functions"]

@@ -31,6 +31,7 @@ SG_OPT_EVAL_PPT = 3
 SG_OPT_EVAL_BLOCKS = 4
 SG_OPT_HIER_KERNEL = 5
 SG_OPT_PROFILE = 6
+SG_OPT_USE_GRAPH = 7
 SG_NUM_PHASES = 3
 
 SG_FN_REFERENCE = 0
@@ -79,6 +80,20 @@ SIGNATURES = {
     "sg_timings": (_i, [_p, _p]),
     "sg_kernel_launches": (_i, [_pi64]),
     "sg_sample_function": (_i, [_p, _i, _p, _i, _p]),
+    "sg_batch_create": (_i, [_i, _p, _p, _p, C.POINTER(_p)]),
+    "sg_batch_destroy": (_i, [_p]),
+    "sg_batch_num_grids": (_i, [_p, _p]),
+    "sg_batch_offsets": (_i, [_p, _p]),
+    "sg_batch_set_values": (_i, [_p, _p]),
+    "sg_batch_set_values_device": (_i, [_p, _p, _p]),
+    "sg_batch_get_values": (_i, [_p, _p]),
+    "sg_batch_sample_function": (_i, [_p, _i, _p, _i, _p]),
+    "sg_batch_hierarchize_async": (_i, [_p, _p]),
+    "sg_batch_hierarchize": (_i, [_p]),
+    "sg_batch_evaluate_device": (_i, [_p, _p, _p, _p, _p]),
+    "sg_batch_sync": (_i, [_p, _p]),
+    "sg_batch_set_option": (_i, [_p, _i, _i64]),
+    "sg_batch_device_bytes": (_i, [_p, _pi64]),
     "sg_last_error": (C.c_char_p, []),
     "sg_version": (C.c_char_p, []),
 }

@@ -7,22 +7,21 @@
 
 #include <stdint.h>
 
+#include <vector_types.h>
+
 #include "sg_kernels.h"
 
-struct EvalArgs {
-    const float *__restrict__ alpha;          /* block layout                 */
-    const float *__restrict__ coords;
-    const int32_t *__restrict__ perm;
-    float *__restrict__ out;
-    int64_t num_evals;
-    int nm1;                                  /* n - 1                        */
-    int regular;                              /* innermost dims unrestricted  */
-    int lim[SG_MAX_DIMS];
-    uint32_t blk3[SG_MAX_LEVELS];             /* block size per budget R      */
-    uint32_t blk2[SG_MAX_LEVELS];             /* sub-block size per budget r  */
-};
+typedef sg_eval_args EvalArgs;
 
 template <int D>
 int eval_launch(const EvalArgs &A, int ppt, void *stream);
+
+/* Points per CTA of the evaluation kernels for `ppt` points per thread. */
+#define SG_EVAL_CTA_POINTS(ppt) (256 * (ppt))
+
+/* Batched form: items[b] = (grid index into `grids`, first point) for CTA b;
+ * every grid of the launch has dimension D. */
+template <int D>
+int eval_batch_launch(const EvalArgs *grids, const int2 *items, int nitems, int ppt, void *stream);
 
 #endif

@@ -2,4 +2,6 @@
 #include "eval_impl.cuh"
 
 template int eval_launch<17>(const EvalArgs &, int, void *);
+template int eval_batch_launch<17>(const EvalArgs *, const int2 *, int, int, void *);
 template int eval_launch<18>(const EvalArgs &, int, void *);
+template int eval_batch_launch<18>(const EvalArgs *, const int2 *, int, int, void *);

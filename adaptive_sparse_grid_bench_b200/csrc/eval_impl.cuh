@@ -295,15 +295,12 @@ struct Walk {
     }
 };
 
+/* Evaluates this thread's points first, first + 32, ..., first + 32(P-1)
+ * (those below `end`) against grid A; sx is this CTA's shared coordinate
+ * buffer. */
 template <int D, int P>
-__global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const EvalArgs A)
+__device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int tid, int64_t first, int64_t end)
 {
-    constexpr int NPX = D >= 4 ? D - 3 : 1; /* prefix coordinates kept in shared memory */
-    __shared__ float sx[NPX * P * kThreads];
-    const int tid = threadIdx.x;
-    const int64_t warp = (blockIdx.x * (int64_t)kThreads + tid) >> 5;
-    const int lane = tid & 31;
-    const int64_t first = warp * (32 * P) + lane;
 
     float xC[P], xA[P], xB[P];
     bool valid[P], nan_in[P];
@@ -311,7 +308,7 @@ __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const E
     for (int p = 0; p < P; ++p) {
         const int64_t i = first + 32 * p;
         float x[D];
-        valid[p] = i < A.num_evals;
+        valid[p] = i < end;
         nan_in[p] = false;
         bool inside = true;
 #pragma unroll
@@ -391,11 +388,43 @@ __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const E
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         const int64_t i = first + 32 * p;
-        if (i < A.num_evals) {
+        if (i < end) {
             const float r = valid[p] ? __fsub_rn(sum[p], comp[p]) : (nan_in[p] ? __int_as_float(0x7fc00000) : 0.0f);
             A.out[A.perm ? A.perm[i] : i] = r;
         }
     }
+}
+
+template <int D, int P>
+__global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const EvalArgs A)
+{
+    constexpr int NPX = D >= 4 ? D - 3 : 1; /* prefix coordinates kept in shared memory */
+    __shared__ float sx[NPX * P * kThreads];
+    const int tid = threadIdx.x;
+    const int64_t warp = (blockIdx.x * (int64_t)kThreads + tid) >> 5;
+    eval_points<D, P>(A, sx, tid, warp * (32 * P) + (tid & 31), A.num_evals);
+}
+
+/* Many grids of the same dimension in one launch: CTA b evaluates the
+ * kThreads*P points of grid items[b].x starting at point items[b].y. */
+template <int D, int P>
+__global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3))
+    k_evaluate_batch(const EvalArgs *__restrict__ grids, const int2 *__restrict__ items)
+{
+    constexpr int NPX = D >= 4 ? D - 3 : 1;
+    __shared__ float sx[NPX * P * kThreads];
+    __shared__ EvalArgs sA;
+    const int tid = threadIdx.x;
+    const int2 item = items[blockIdx.x];
+    {
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(grids + item.x);
+        uint32_t *dst = reinterpret_cast<uint32_t *>(&sA);
+        for (int w = tid; w < (int)(sizeof(EvalArgs) / 4); w += kThreads) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int64_t start = item.y;
+    const int64_t end = min(start + (int64_t)kThreads * P, sA.num_evals);
+    eval_points<D, P>(sA, sx, tid, start + (tid >> 5) * (32 * P) + (tid & 31), end);
 }
 
 template <int D, int P>
@@ -416,6 +445,18 @@ int eval_launch(const EvalArgs &A, int ppt, void *stream)
 {
     if (ppt == 1) return sgeval::launch_eval<D, 1>(A, stream);
     return sgeval::launch_eval<D, 2>(A, stream);
+}
+
+template <int D>
+int eval_batch_launch(const EvalArgs *grids, const int2 *items, int nitems, int ppt, void *stream)
+{
+    if (nitems <= 0) return cudaSuccess;
+    if (ppt == 1)
+        sgeval::k_evaluate_batch<D, 1><<<nitems, sgeval::kThreads, 0, (cudaStream_t)stream>>>(grids, items);
+    else
+        sgeval::k_evaluate_batch<D, 2><<<nitems, sgeval::kThreads, 0, (cudaStream_t)stream>>>(grids, items);
+    sgk_count(1);
+    return cudaGetLastError();
 }
 
 #endif

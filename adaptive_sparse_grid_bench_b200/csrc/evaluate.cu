@@ -189,29 +189,49 @@ int scan_exclusive(uint32_t *v, int64_t m, uint32_t *tmp, cudaStream_t st)
 
 extern "C" {
 
+void sgk_fill_eval_args(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
+                        int64_t num_evals, sg_eval_args *A)
+{
+    A->alpha = p->alpha;
+    A->coords = coords;
+    A->perm = perm;
+    A->out = out;
+    A->num_evals = num_evals;
+    A->nm1 = p->n - 1;
+    for (int k = 0; k < SG_MAX_DIMS; ++k) A->lim[k] = k < p->d ? p->lim[k] : 0;
+    for (int r = 0; r < SG_MAX_LEVELS; ++r) {
+        A->blk3[r] = p->blk3[r];
+        A->blk2[r] = p->blk2[r];
+    }
+    bool reg = true;
+    for (int k = p->d >= 3 ? p->d - 3 : 0; k < p->d; ++k) reg = reg && p->lim[k] >= p->n - 1;
+    A->regular = reg;
+}
+
 int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
                  int64_t num_evals, void *stream)
 {
     if (num_evals <= 0) return cudaSuccess;
     EvalArgs A;
-    A.alpha = p->alpha;
-    A.coords = coords;
-    A.perm = perm;
-    A.out = out;
-    A.num_evals = num_evals;
-    A.nm1 = p->n - 1;
-    for (int k = 0; k < SG_MAX_DIMS; ++k) A.lim[k] = k < p->d ? p->lim[k] : 0;
-    for (int r = 0; r < SG_MAX_LEVELS; ++r) {
-        A.blk3[r] = p->blk3[r];
-        A.blk2[r] = p->blk2[r];
-    }
-    bool reg = true;
-    for (int k = p->d >= 3 ? p->d - 3 : 0; k < p->d; ++k) reg = reg && p->lim[k] >= p->n - 1;
-    A.regular = reg;
+    sgk_fill_eval_args(p, coords, perm, out, num_evals, &A);
     const int ppt = p->ppt;
     switch (p->d) {
 #define SG_D(DD) \
     case DD: return eval_launch<DD>(A, ppt, stream);
+        SG_D(1) SG_D(2) SG_D(3) SG_D(4) SG_D(5) SG_D(6) SG_D(7) SG_D(8) SG_D(9) SG_D(10)
+        SG_D(11) SG_D(12) SG_D(13) SG_D(14) SG_D(15) SG_D(16) SG_D(17) SG_D(18) SG_D(19)
+        SG_D(20)
+#undef SG_D
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, int nitems, int ppt, void *stream)
+{
+    const int2 *it = reinterpret_cast<const int2 *>(items);
+    switch (d) {
+#define SG_D(DD) \
+    case DD: return eval_batch_launch<DD>(grids, it, nitems, ppt, stream);
         SG_D(1) SG_D(2) SG_D(3) SG_D(4) SG_D(5) SG_D(6) SG_D(7) SG_D(8) SG_D(9) SG_D(10)
         SG_D(11) SG_D(12) SG_D(13) SG_D(14) SG_D(15) SG_D(16) SG_D(17) SG_D(18) SG_D(19)
         SG_D(20)

@@ -1,0 +1,55 @@
+/* Internal state of a grid batch (sgrid_batch.c). */
+#ifndef SG_BATCH_INTERNAL_H
+#define SG_BATCH_INTERNAL_H
+
+#include <cuda_runtime_api.h>
+#include <stdarg.h>
+#include <stdint.h>
+
+#include "sg_kernels.h"
+#include "sg_layout.h"
+
+#define SG_BATCH_CLASSES 4 /* size classes of the shared-memory hierarchization */
+
+struct sg_batch {
+    int ng;
+    sg_layout *L;        /* per grid                                              */
+    int64_t *voff;       /* compact value offsets (caller's concatenation), ng+1   */
+    int64_t *doff;       /* offsets in the device value buffer (32-aligned), ng+1  */
+    int64_t *boff;       /* offsets in the block-layout buffer, ng+1               */
+    int dev, has_values, eval_dirty;
+    int precision, ppt, use_graph;
+    int64_t dev_bytes;
+    float *d_alpha;      /* all grids, group-aligned layout                       */
+    double *d_work;      /* FP64 sweep values (lazy)                              */
+    float *d_blk;        /* all grids, block layout                               */
+    int *d_err;
+    /* shared-memory path */
+    int n_smem;
+    int cls_first[SG_BATCH_CLASSES], cls_count[SG_BATCH_CLASSES], cls_max_npad[SG_BATCH_CLASSES];
+    sg_smem_grid *d_smem_grids;
+    sg_chain *d_smem_chains;
+    uint32_t *d_smem_seg;
+    /* chain-sweep path */
+    int has_sweep_grids;
+    sg_sweep_tables sweepB[SG_MAX_DIMS];
+    sg_chain *d_chB[SG_MAX_DIMS];
+    uint32_t *d_segB[SG_MAX_DIMS];
+    /* evaluation */
+    sg_repack *d_repack;
+    int64_t nrepack;
+    sg_eval_args *h_eval_args, *d_eval_args;
+    int32_t *h_items, *d_items;
+    int64_t items_cap;
+    int items_first[SG_MAX_DIMS + 1], items_count[SG_MAX_DIMS + 1];
+    int64_t *eval_pt_off;
+    const float *eval_coords;
+    float *eval_out;
+    int eval_ppt;
+    cudaGraphExec_t hier_graph, eval_graph;
+};
+
+/* Sets the calling thread's sg_last_error() text (sgrid.c). */
+void sg_set_error(const char *fmt, va_list ap);
+
+#endif

@@ -48,13 +48,49 @@ typedef struct sg_eval_plan {
     int ppt;                     /* points per thread (1 or 2)               */
 } sg_eval_plan;
 
+/* Per-grid arguments of the evaluation kernels (also the element type of
+ * the batched launch's grid table). */
+typedef struct sg_eval_args {
+    const float *alpha;      /* block layout                         */
+    const float *coords;     /* num_evals x d                        */
+    const int32_t *perm;     /* optional: sorted position -> caller  */
+    float *out;
+    int64_t num_evals;
+    int nm1;                 /* n - 1                                */
+    int regular;             /* innermost dims unrestricted          */
+    int lim[SG_MAX_DIMS];
+    uint32_t blk3[SG_MAX_LEVELS]; /* block size per budget R         */
+    uint32_t blk2[SG_MAX_LEVELS]; /* sub-block size per budget r     */
+} sg_eval_args;
+
+void sgk_fill_eval_args(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
+                        int64_t num_evals, sg_eval_args *a);
+
+/* out[perm ? perm[i] : i] = interpolant at coords[i*d .. i*d+d-1]. */
+int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
+                 int64_t num_evals, void *stream);
+/* Many grids of dimension d in one launch: items (device, 2 ints per CTA) =
+ * (index into grids, first point); each CTA covers SG_EVAL_CTA_POINTS(ppt)
+ * points of its grid. */
+int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, int nitems, int ppt,
+                       void *stream);
+
 /* Reorders the surpluses from the group-aligned compact layout into the
  * block layout (one descriptor per subspace). */
 int sgk_repack(const float *src, float *dst, const sg_repack *rp, int64_t nsub, void *stream);
 
-/* out[perm ? perm[i] : i] = interpolant at coords[i*d .. i*d+d-1]. */
-int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm,
-                 float *out, int64_t num_evals, void *stream);
+/* Whole-grid hierarchization in shared memory for small grids, one CTA per
+ * grid (all d sweeps between one load and one store). */
+typedef struct sg_smem_grid {
+    uint32_t base;                  /* first element in the value buffer (multiple of 32) */
+    uint32_t npad;                  /* elements (multiple of 32)                         */
+    int d;
+    uint32_t chain0[SG_MAX_DIMS];   /* first chain of sweep k in the chain array          */
+    uint32_t nch[SG_MAX_DIMS];      /* chains of sweep k                                  */
+} sg_smem_grid;
+#define SG_SMEM_GRID_MAX_BYTES (200 * 1024)
+int sgk_hier_smem_grids(float *a, const sg_smem_grid *grids, int ngrids, const sg_chain *chains,
+                        const uint32_t *seg, int max_npad, int fp64, void *stream);
 
 /* Spatial ordering of query points: writes the sorted coordinates and the
  * permutation (sorted position -> caller position).  scratch: device bytes

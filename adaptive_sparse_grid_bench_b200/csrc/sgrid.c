@@ -12,6 +12,7 @@
 #include <string.h>
 
 #include "sg_kernels.h"
+#include "sg_batch_internal.h"
 #include "sg_layout.h"
 
 #define SG_API __attribute__((visibility("default")))
@@ -46,11 +47,13 @@ struct sg_grid {
 
 static __thread char g_err[512];
 
+void sg_set_error(const char *fmt, va_list ap) { vsnprintf(g_err, sizeof(g_err), fmt, ap); }
+
 static int fail(int code, const char *fmt, ...)
 {
     va_list ap;
     va_start(ap, fmt);
-    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    sg_set_error(fmt, ap);
     va_end(ap);
     return code;
 }

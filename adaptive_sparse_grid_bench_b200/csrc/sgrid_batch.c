@@ -1,0 +1,703 @@
+/*
+ * Batches of independent grids (sg_batch_* in include/sgrid.h).  Host code in
+ * C.  A batch holds many grids of mixed d, n and limits in one device buffer
+ * (each grid in the group-aligned compact layout, 32-element aligned), and
+ * runs all of them through a fixed set of launches:
+ *   hierarchize: grids that fit in shared memory (n <= 9, <= 200 KB) are
+ *     hierarchized whole, one CTA per grid, in a few size classes; the
+ *     others share one chain-sweep launch per sweep index k across grids
+ *     (sweeps of different grids are independent);
+ *   evaluate: the surpluses are repacked into the block layout by one launch
+ *     over all subspaces of all grids, then one evaluation launch per
+ *     distinct d covers every grid of that d, 256*ppt points per CTA.
+ * Both sequences can be captured once in a CUDA graph and replayed.
+ */
+#include <cuda_runtime_api.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "sg_batch_internal.h"
+#include "sg_kernels.h"
+#include "sg_layout.h"
+
+#define SG_API __attribute__((visibility("default")))
+
+/* size classes of the shared-memory path (bytes of the larger of FP32/FP64) */
+static const int64_t k_class_bytes[SG_BATCH_CLASSES] = {8 * 1024, 32 * 1024, 96 * 1024, SG_SMEM_GRID_MAX_BYTES};
+
+static int bfail(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    sg_set_error(fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+static int bcuda(cudaError_t e, const char *what)
+{
+    return bfail(SG_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define BCU(call, what)                                   \
+    do {                                                  \
+        cudaError_t e_ = (call);                          \
+        if (e_ != cudaSuccess) return bcuda(e_, what);    \
+    } while (0)
+
+SG_API int sg_batch_create(int num_grids, const int *dims, const int *levels, const int *limits,
+                           sg_batch **out)
+{
+    sg_batch *b;
+    int g, r;
+    int64_t lim_at = 0, doff = 0, voff = 0;
+    if (!out || num_grids < 1 || !dims || !levels) return bfail(SG_ERR_ARG, "sg_batch_create: bad argument");
+    *out = NULL;
+    b = (sg_batch *)calloc(1, sizeof(sg_batch));
+    if (!b) return bfail(SG_ERR_NOMEM, "sg_batch_create: out of host memory");
+    b->ng = num_grids;
+    b->L = (sg_layout *)calloc((size_t)num_grids, sizeof(sg_layout));
+    b->voff = (int64_t *)calloc((size_t)num_grids + 1, sizeof(int64_t));
+    b->doff = (int64_t *)calloc((size_t)num_grids + 1, sizeof(int64_t));
+    b->boff = (int64_t *)calloc((size_t)num_grids + 1, sizeof(int64_t));
+    if (!b->L || !b->voff || !b->doff || !b->boff) {
+        sg_batch_destroy(b);
+        return bfail(SG_ERR_NOMEM, "sg_batch_create: out of host memory");
+    }
+    for (g = 0; g < num_grids; g++) {
+        r = sg_layout_init(&b->L[g], dims[g], levels[g], limits ? limits + lim_at : NULL);
+        if (r != SG_OK) {
+            sg_batch_destroy(b);
+            return bfail(r, "sg_batch_create: grid %d (d=%d n=%d) rejected", g, dims[g], levels[g]);
+        }
+        lim_at += dims[g];
+        b->voff[g] = voff;
+        b->doff[g] = doff;
+        b->boff[g] = voff;
+        voff += b->L[g].N;
+        doff += b->L[g].Npad;
+    }
+    b->voff[num_grids] = voff;
+    b->doff[num_grids] = doff;
+    b->boff[num_grids] = voff;
+    if (doff >= ((int64_t)1 << 32) - 64) {
+        sg_batch_destroy(b);
+        return bfail(SG_ERR_RANGE, "sg_batch_create: %lld values exceed 32-bit offsets", (long long)doff);
+    }
+    b->dev = -1;
+    b->ppt = 2;
+    b->precision = SG_HIER_FP32;
+    b->use_graph = 1;
+    *out = b;
+    return SG_OK;
+}
+
+static void free_dev(sg_batch *b)
+{
+    int k;
+    if (b->dev < 0) return;
+    cudaSetDevice(b->dev);
+    if (b->hier_graph) cudaGraphExecDestroy(b->hier_graph);
+    if (b->eval_graph) cudaGraphExecDestroy(b->eval_graph);
+    b->hier_graph = b->eval_graph = NULL;
+    cudaFree(b->d_alpha);
+    cudaFree(b->d_work);
+    cudaFree(b->d_blk);
+    cudaFree(b->d_repack);
+    cudaFree(b->d_smem_grids);
+    cudaFree(b->d_smem_chains);
+    cudaFree(b->d_smem_seg);
+    for (k = 0; k < SG_MAX_DIMS; k++) {
+        cudaFree(b->d_chB[k]);
+        cudaFree(b->d_segB[k]);
+    }
+    cudaFree(b->d_eval_args);
+    cudaFree(b->d_items);
+    cudaFree(b->d_err);
+    free(b->h_eval_args);
+    free(b->h_items);
+    b->h_eval_args = NULL;
+    b->h_items = NULL;
+}
+
+SG_API int sg_batch_destroy(sg_batch *b)
+{
+    if (!b) return SG_OK;
+    free_dev(b);
+    free(b->L);
+    free(b->voff);
+    free(b->doff);
+    free(b->boff);
+    free(b->eval_pt_off);
+    free(b);
+    return SG_OK;
+}
+
+SG_API int sg_batch_offsets(const sg_batch *b, int64_t *value_offsets)
+{
+    int g;
+    if (!b || !value_offsets) return bfail(SG_ERR_ARG, "sg_batch_offsets: NULL argument");
+    for (g = 0; g <= b->ng; g++) value_offsets[g] = b->voff[g];
+    return SG_OK;
+}
+
+SG_API int sg_batch_num_grids(const sg_batch *b, int *num_grids)
+{
+    if (!b || !num_grids) return bfail(SG_ERR_ARG, "sg_batch_num_grids: NULL argument");
+    *num_grids = b->ng;
+    return SG_OK;
+}
+
+static int balloc(sg_batch *b, void **p, int64_t bytes, const char *what)
+{
+    cudaError_t e = cudaMalloc(p, (size_t)(bytes > 0 ? bytes : 16));
+    if (e != cudaSuccess) {
+        *p = NULL;
+        cudaGetLastError();
+        return bfail(e == cudaErrorMemoryAllocation ? SG_ERR_NOMEM : SG_ERR_CUDA, "cudaMalloc(%lld) for %s: %s",
+                     (long long)bytes, what, cudaGetErrorString(e));
+    }
+    b->dev_bytes += bytes;
+    return SG_OK;
+}
+
+static int upload(sg_batch *b, void **dst, const void *src, int64_t bytes, const char *what)
+{
+    int r = balloc(b, dst, bytes, what);
+    if (r != SG_OK) return r;
+    if (bytes > 0) BCU(cudaMemcpy(*dst, src, (size_t)bytes, cudaMemcpyHostToDevice), what);
+    return SG_OK;
+}
+
+/* grids that take the shared-memory path, and their size class */
+static int smem_class(const sg_layout *L)
+{
+    int c;
+    const int64_t bytes = L->Npad * 8; /* sized for FP64 so both precisions fit */
+    if (L->n > 9) return -1;
+    for (c = 0; c < SG_BATCH_CLASSES; c++)
+        if (bytes <= k_class_bytes[c]) return c;
+    return -1;
+}
+
+static int cmp_by_size_desc(const void *x, const void *y, void *ctx)
+{
+    const sg_batch *b = (const sg_batch *)ctx;
+    const int gx = *(const int *)x, gy = *(const int *)y;
+    if (b->L[gx].Npad != b->L[gy].Npad) return b->L[gx].Npad > b->L[gy].Npad ? -1 : 1;
+    return gx - gy;
+}
+
+static int materialize(sg_batch *b)
+{
+    int g, k, c, r = SG_OK;
+    int *order = NULL;
+    sg_smem_grid *sg = NULL;
+    sg_chain *sch = NULL;
+    uint32_t *sseg = NULL;
+    int64_t nsg = 0, nsch = 0, nsseg = 0, cap_sch = 0, cap_sseg = 0;
+    sg_chain *chB[SG_MAX_DIMS];
+    uint32_t *segB[SG_MAX_DIMS];
+    int64_t nchB[SG_MAX_DIMS], nsegB[SG_MAX_DIMS], capchB[SG_MAX_DIMS], capsegB[SG_MAX_DIMS];
+    sg_repack *rp = NULL;
+    int64_t nrp = 0;
+    if (b->dev >= 0) return SG_OK;
+    memset(chB, 0, sizeof(chB));
+    memset(segB, 0, sizeof(segB));
+    memset(nchB, 0, sizeof(nchB));
+    memset(nsegB, 0, sizeof(nsegB));
+    memset(capchB, 0, sizeof(capchB));
+    memset(capsegB, 0, sizeof(capsegB));
+    BCU(cudaGetDevice(&b->dev), "cudaGetDevice");
+    if ((r = balloc(b, (void **)&b->d_alpha, b->doff[b->ng] * 4, "batch values")) != SG_OK) goto done;
+    BCU(cudaMemset(b->d_alpha, 0, (size_t)b->doff[b->ng] * 4), "cudaMemset");
+    if ((r = balloc(b, (void **)&b->d_blk, b->boff[b->ng] * 4, "batch block layout")) != SG_OK) goto done;
+    if ((r = balloc(b, (void **)&b->d_err, 16, "error flag")) != SG_OK) goto done;
+    BCU(cudaMemset(b->d_err, 0, 16), "cudaMemset");
+
+    /* shared-memory path: grids in size classes, largest first inside each */
+    order = (int *)malloc((size_t)b->ng * sizeof(int));
+    sg = (sg_smem_grid *)calloc((size_t)b->ng, sizeof(sg_smem_grid));
+    if (!order || !sg) { r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
+    for (g = 0; g < b->ng; g++) order[g] = g;
+    qsort_r(order, (size_t)b->ng, sizeof(int), cmp_by_size_desc, b);
+    for (c = SG_BATCH_CLASSES - 1; c >= 0; c--) {
+        b->cls_first[c] = (int)nsg;
+        b->cls_max_npad[c] = 0;
+        for (int q = 0; q < b->ng; q++) {
+            const int gg = order[q];
+            const sg_layout *L = &b->L[gg];
+            if (smem_class(L) != c) continue;
+            sg[nsg].base = (uint32_t)b->doff[gg];
+            sg[nsg].npad = (uint32_t)L->Npad;
+            sg[nsg].d = L->d;
+            if ((int)L->Npad > b->cls_max_npad[c]) b->cls_max_npad[c] = (int)L->Npad;
+            for (k = 0; k < L->d; k++) {
+                sg_chain *ch = NULL;
+                uint32_t *sgo = NULL;
+                int64_t nch = 0, nseg = 0, i;
+                if ((r = sg_layout_chains(L, k, &ch, &nch, &sgo, &nseg)) != SG_OK) goto done;
+                while (nsch + nch > cap_sch) {
+                    cap_sch = cap_sch ? 2 * cap_sch : 4096;
+                    sch = (sg_chain *)realloc(sch, (size_t)cap_sch * sizeof(sg_chain));
+                }
+                while (nsseg + nseg > cap_sseg) {
+                    cap_sseg = cap_sseg ? 2 * cap_sseg : 16384;
+                    sseg = (uint32_t *)realloc(sseg, (size_t)cap_sseg * sizeof(uint32_t));
+                }
+                if (!sch || !sseg) { free(ch); free(sgo); r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
+                sg[nsg].chain0[k] = (uint32_t)nsch;
+                sg[nsg].nch[k] = (uint32_t)nch;
+                for (i = 0; i < nch; i++) {
+                    sch[nsch + i] = ch[i];
+                    sch[nsch + i].seg = (uint32_t)(ch[i].seg + nsseg);
+                }
+                /* offsets relative to the grid: the shared-memory copy of a
+                 * grid has its device layout */
+                for (i = 0; i < nseg; i++) sseg[nsseg + i] = sgo[i];
+                nsch += nch;
+                nsseg += nseg;
+                free(ch);
+                free(sgo);
+            }
+            nsg++;
+        }
+        b->cls_count[c] = (int)nsg - b->cls_first[c];
+    }
+    b->n_smem = (int)nsg;
+    if ((r = upload(b, (void **)&b->d_smem_grids, sg, nsg * (int64_t)sizeof(sg_smem_grid), "batch grid table")) != SG_OK) goto done;
+    if ((r = upload(b, (void **)&b->d_smem_chains, sch, nsch * (int64_t)sizeof(sg_chain), "batch chains")) != SG_OK) goto done;
+    if ((r = upload(b, (void **)&b->d_smem_seg, sseg, nsseg * 4, "batch segments")) != SG_OK) goto done;
+
+    /* chain-sweep path: sweep k of every other grid in one launch */
+    for (g = 0; g < b->ng; g++) {
+        const sg_layout *L = &b->L[g];
+        if (smem_class(L) >= 0) continue;
+        b->has_sweep_grids = 1;
+        for (k = 0; k < L->d; k++) {
+            sg_chain *ch = NULL;
+            uint32_t *sgo = NULL;
+            int64_t nch = 0, nseg = 0, i;
+            if ((r = sg_layout_chains(L, k, &ch, &nch, &sgo, &nseg)) != SG_OK) goto done;
+            while (nchB[k] + nch > capchB[k]) {
+                capchB[k] = capchB[k] ? 2 * capchB[k] : 4096;
+                chB[k] = (sg_chain *)realloc(chB[k], (size_t)capchB[k] * sizeof(sg_chain));
+            }
+            while (nsegB[k] + nseg > capsegB[k]) {
+                capsegB[k] = capsegB[k] ? 2 * capsegB[k] : 16384;
+                segB[k] = (uint32_t *)realloc(segB[k], (size_t)capsegB[k] * sizeof(uint32_t));
+            }
+            if (!chB[k] || !segB[k]) { free(ch); free(sgo); r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
+            for (i = 0; i < nch; i++) {
+                int j;
+                int64_t e32 = 0, e64 = 0;
+                chB[k][nchB[k] + i] = ch[i];
+                chB[k][nchB[k] + i].seg = (uint32_t)(ch[i].seg + nsegB[k]);
+                for (j = 0; j <= ch[i].lmax; j++) {
+                    int64_t sz = (int64_t)1 << (ch[i].sigma + j);
+                    e32 += sz < 4 ? 4 : sz;
+                    e64 += sz < 2 ? 2 : sz;
+                }
+                if (e32 > b->sweepB[k].cap32) b->sweepB[k].cap32 = e32;
+                if (e64 > b->sweepB[k].cap64) b->sweepB[k].cap64 = e64;
+                if (ch[i].lmax > b->sweepB[k].lmax_max) b->sweepB[k].lmax_max = ch[i].lmax;
+            }
+            for (i = 0; i < nseg; i++) segB[k][nsegB[k] + i] = (uint32_t)(sgo[i] + b->doff[g]);
+            nchB[k] += nch;
+            nsegB[k] += nseg;
+            free(ch);
+            free(sgo);
+        }
+    }
+    for (k = 0; k < SG_MAX_DIMS; k++) {
+        if ((r = upload(b, (void **)&b->d_chB[k], chB[k], nchB[k] * (int64_t)sizeof(sg_chain), "sweep chains")) != SG_OK)
+            goto done;
+        if ((r = upload(b, (void **)&b->d_segB[k], segB[k], nsegB[k] * 4, "sweep segments")) != SG_OK) goto done;
+        b->sweepB[k].chains = b->d_chB[k];
+        b->sweepB[k].seg = b->d_segB[k];
+        b->sweepB[k].nchains = nchB[k];
+    }
+
+    /* evaluation: repack table over all grids, per-grid block sizes */
+    for (g = 0; g < b->ng; g++) nrp += b->L[g].S;
+    rp = (sg_repack *)malloc((size_t)nrp * sizeof(sg_repack));
+    if (!rp) { r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
+    nrp = 0;
+    for (g = 0; g < b->ng; g++) {
+        sg_repack *one = NULL;
+        uint32_t blk3[SG_MAX_LEVELS], blk2[SG_MAX_LEVELS];
+        int64_t i;
+        if ((r = sg_layout_eval_tables(&b->L[g], &one, blk3, blk2)) != SG_OK) goto done;
+        for (i = 0; i < b->L[g].S; i++) {
+            rp[nrp + i] = one[i];
+            rp[nrp + i].src = (uint32_t)(one[i].src + b->doff[g]);
+            rp[nrp + i].dst = (uint32_t)(one[i].dst + b->boff[g]);
+        }
+        nrp += b->L[g].S;
+        free(one);
+    }
+    b->nrepack = nrp;
+    r = upload(b, (void **)&b->d_repack, rp, nrp * (int64_t)sizeof(sg_repack), "batch repack table");
+done:
+    free(order);
+    free(sg);
+    free(sch);
+    free(sseg);
+    free(rp);
+    for (k = 0; k < SG_MAX_DIMS; k++) {
+        free(chB[k]);
+        free(segB[k]);
+    }
+    if (r != SG_OK) {
+        free_dev(b);
+        b->dev = -1;
+    }
+    return r;
+}
+
+static int enter(sg_batch *b, int *prev)
+{
+    BCU(cudaGetDevice(prev), "cudaGetDevice");
+    if (b->dev >= 0 && b->dev != *prev) BCU(cudaSetDevice(b->dev), "cudaSetDevice");
+    return SG_OK;
+}
+
+static void leave(sg_batch *b, int prev)
+{
+    if (b->dev >= 0 && b->dev != prev) cudaSetDevice(prev);
+}
+
+static int copy_values(sg_batch *b, float *dst, const float *src, int to_dev, enum cudaMemcpyKind kind, cudaStream_t st)
+{
+    int g, s;
+    for (g = 0; g < b->ng; g++) {
+        const sg_layout *L = &b->L[g];
+        for (s = 0; s < L->n; s++) {
+            const int64_t cnt = L->lidx[s + 1] - L->lidx[s];
+            const int64_t c_off = b->voff[g] + L->lidx[s], d_off = b->doff[g] + L->plidx[s];
+            if (cnt == 0) continue;
+            BCU(cudaMemcpyAsync(to_dev ? dst + d_off : dst + c_off, to_dev ? src + c_off : src + d_off,
+                                (size_t)cnt * 4, kind, st),
+                "batch value copy");
+        }
+    }
+    return SG_OK;
+}
+
+SG_API int sg_batch_set_values(sg_batch *b, const float *values)
+{
+    int prev, r;
+    if (!b || !values) return bfail(SG_ERR_ARG, "sg_batch_set_values: NULL argument");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    if ((r = materialize(b)) == SG_OK && (r = copy_values(b, b->d_alpha, values, 1, cudaMemcpyHostToDevice, 0)) == SG_OK) {
+        cudaError_t e = cudaStreamSynchronize(0);
+        if (e != cudaSuccess) r = bcuda(e, "sg_batch_set_values");
+        else b->has_values = 1, b->eval_dirty = 1;
+    }
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_set_values_device(sg_batch *b, const float *values, void *stream)
+{
+    int prev, r;
+    if (!b || !values) return bfail(SG_ERR_ARG, "sg_batch_set_values_device: NULL argument");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    if ((r = materialize(b)) == SG_OK &&
+        (r = copy_values(b, b->d_alpha, values, 1, cudaMemcpyDeviceToDevice, (cudaStream_t)stream)) == SG_OK)
+        b->has_values = 1, b->eval_dirty = 1;
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_get_values(sg_batch *b, float *values)
+{
+    int prev, r;
+    if (!b || !values) return bfail(SG_ERR_ARG, "sg_batch_get_values: NULL argument");
+    if (!b->has_values) return bfail(SG_ERR_STATE, "sg_batch_get_values: no values have been set");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    if ((r = copy_values(b, values, b->d_alpha, 0, cudaMemcpyDeviceToHost, 0)) == SG_OK) {
+        cudaError_t e = cudaStreamSynchronize(0);
+        if (e != cudaSuccess) r = bcuda(e, "sg_batch_get_values");
+    }
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_sample_function(sg_batch *b, int fn, const double *params, int params_per_grid, void *stream)
+{
+    int prev, r, g, e;
+    if (!b || params_per_grid < 0 || params_per_grid > SG_MAX_FN_PARAMS || (params_per_grid > 0 && !params))
+        return bfail(SG_ERR_ARG, "sg_batch_sample_function: bad argument");
+    if (fn < SG_FN_REFERENCE || fn > SG_FN_QUAD) return bfail(SG_ERR_ARG, "sg_batch_sample_function: unknown function");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    if ((r = materialize(b)) == SG_OK) {
+        for (g = 0; g < b->ng && r == SG_OK; g++) {
+            const int need = fn == SG_FN_BUMP ? 2 : (fn == SG_FN_QUAD ? 3 * b->L[g].d : 0);
+            if (params_per_grid < need) {
+                r = bfail(SG_ERR_ARG, "sg_batch_sample_function: grid %d needs %d parameters", g, need);
+                break;
+            }
+            e = sgk_sample(&b->L[g], fn, params ? params + (size_t)g * params_per_grid : NULL, params_per_grid,
+                           b->d_alpha + b->doff[g], stream);
+            if (e != cudaSuccess) r = bcuda((cudaError_t)e, "sg_batch_sample_function");
+        }
+        if (r == SG_OK) b->has_values = 1, b->eval_dirty = 1;
+    }
+    leave(b, prev);
+    return r;
+}
+
+/* The hierarchization launches (also what the graph captures). */
+static int hier_launches(sg_batch *b, cudaStream_t st)
+{
+    int k, c, e;
+    const int fp64 = b->precision == SG_HIER_FP64;
+    if (b->has_sweep_grids) {
+        if (fp64) {
+            if ((e = sgk_widen(b->d_alpha, b->d_work, b->doff[b->ng], st)) != cudaSuccess) return bcuda((cudaError_t)e, "widen");
+            for (k = 0; k < SG_MAX_DIMS; k++) {
+                if (!b->sweepB[k].nchains) continue;
+                e = sgk_chain_smem_bytes(b->sweepB[k].cap64, 8) >= 0
+                        ? sgk_sweep_chains_f64(b->d_work, &b->sweepB[k], b->d_err, st)
+                        : sgk_sweep_gather_f64(b->d_work, &b->sweepB[k], st);
+                if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch FP64 sweep");
+            }
+            if ((e = sgk_narrow(b->d_work, b->d_alpha, b->doff[b->ng], st)) != cudaSuccess) return bcuda((cudaError_t)e, "narrow");
+        } else {
+            for (k = 0; k < SG_MAX_DIMS; k++) {
+                if (!b->sweepB[k].nchains) continue;
+                e = sgk_chain_smem_bytes(b->sweepB[k].cap32, 4) >= 0
+                        ? sgk_sweep_chains_f32(b->d_alpha, &b->sweepB[k], b->d_err, st)
+                        : sgk_sweep_gather_f32(b->d_alpha, &b->sweepB[k], st);
+                if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch FP32 sweep");
+            }
+        }
+    }
+    /* after the sweeps: their FP64 round trip rewrites the whole buffer with
+     * the (unchanged) nodal values of the shared-memory grids */
+    for (c = 0; c < SG_BATCH_CLASSES; c++) {
+        if (!b->cls_count[c]) continue;
+        e = sgk_hier_smem_grids(b->d_alpha, b->d_smem_grids + b->cls_first[c], b->cls_count[c], b->d_smem_chains,
+                                b->d_smem_seg, b->cls_max_npad[c], fp64, st);
+        if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch shared-memory hierarchization");
+    }
+    return SG_OK;
+}
+
+static int run_graph(cudaGraphExec_t *exec, int (*body)(sg_batch *, cudaStream_t), sg_batch *b, cudaStream_t st)
+{
+    cudaGraph_t graph = NULL;
+    cudaError_t e;
+    int r;
+    if (*exec) {
+        BCU(cudaGraphLaunch(*exec, st), "cudaGraphLaunch");
+        return SG_OK;
+    }
+    if (st == 0) return body(b, st); /* the legacy stream cannot be captured */
+    BCU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    r = body(b, st);
+    e = cudaStreamEndCapture(st, &graph);
+    if (r != SG_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return r;
+    }
+    if (e != cudaSuccess) return bcuda(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        *exec = NULL;
+        return bcuda(e, "cudaGraphInstantiate");
+    }
+    BCU(cudaGraphLaunch(*exec, st), "cudaGraphLaunch");
+    return SG_OK;
+}
+
+SG_API int sg_batch_hierarchize_async(sg_batch *b, void *stream)
+{
+    int prev, r;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!b) return bfail(SG_ERR_ARG, "sg_batch_hierarchize_async: NULL batch");
+    if (!b->has_values) return bfail(SG_ERR_STATE, "sg_batch_hierarchize: no values have been set");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    if (b->precision == SG_HIER_FP64 && b->has_sweep_grids && !b->d_work)
+        r = balloc(b, (void **)&b->d_work, b->doff[b->ng] * 8, "batch FP64 working values");
+    if (r == SG_OK) r = b->use_graph ? run_graph(&b->hier_graph, hier_launches, b, st) : hier_launches(b, st);
+    b->eval_dirty = 1;
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_sync(sg_batch *b, void *stream)
+{
+    int prev, r = SG_OK, flag = 0;
+    cudaError_t e;
+    if (!b) return bfail(SG_ERR_ARG, "sg_batch_sync: NULL batch");
+    if (b->dev < 0) return SG_OK;
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    e = cudaStreamSynchronize((cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaMemcpy(&flag, b->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) r = bcuda(e, "sg_batch_sync");
+    else if (flag) {
+        cudaMemset(b->d_err, 0, sizeof(int));
+        r = bfail(SG_ERR_TIMEOUT, "a device-side wait gave up; the batch values are not valid");
+    }
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_hierarchize(sg_batch *b)
+{
+    int r = sg_batch_hierarchize_async(b, 0);
+    return r == SG_OK ? sg_batch_sync(b, 0) : r;
+}
+
+/* Evaluation plan: per-grid kernel arguments and per-dimension CTA items for
+ * the caller's point offsets and buffers (kept, so an identical call replays
+ * the captured graph). */
+static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, float *out)
+{
+    int g, k, r;
+    int64_t coff = 0, ni = 0, cap_items = 0;
+    const int cta = 256 * b->ppt;
+    int same = b->h_eval_args && b->eval_coords == coords && b->eval_out == out && b->eval_ppt == b->ppt;
+    for (g = 0; same && g <= b->ng; g++) same = b->eval_pt_off[g] == pt_off[g];
+    if (same) return SG_OK;
+    if (b->eval_graph) {
+        cudaGraphExecDestroy(b->eval_graph);
+        b->eval_graph = NULL;
+    }
+    if (!b->h_eval_args) {
+        b->h_eval_args = (sg_eval_args *)calloc((size_t)b->ng, sizeof(sg_eval_args));
+        b->eval_pt_off = (int64_t *)calloc((size_t)b->ng + 1, sizeof(int64_t));
+        if (!b->h_eval_args || !b->eval_pt_off) return bfail(SG_ERR_NOMEM, "out of host memory");
+        if ((r = balloc(b, (void **)&b->d_eval_args, b->ng * (int64_t)sizeof(sg_eval_args), "batch eval args")) != SG_OK)
+            return r;
+    }
+    for (k = 0; k <= SG_MAX_DIMS; k++) b->items_first[k] = b->items_count[k] = 0;
+    for (g = 0; g < b->ng; g++) {
+        const int64_t m = pt_off[g + 1] - pt_off[g];
+        if (m < 0) return bfail(SG_ERR_ARG, "sg_batch_evaluate: point offsets decrease at grid %d", g);
+        cap_items += (m + cta - 1) / cta;
+    }
+    free(b->h_items);
+    b->h_items = (int32_t *)malloc((size_t)(cap_items > 0 ? cap_items : 1) * 2 * sizeof(int32_t));
+    if (!b->h_items) return bfail(SG_ERR_NOMEM, "out of host memory");
+    for (g = 0; g < b->ng; g++) {
+        const sg_layout *L = &b->L[g];
+        sg_eval_plan p;
+        sg_eval_shape sh;
+        sg_eval_sub sub;
+        int s;
+        p.alpha = b->d_blk + b->boff[g];
+        p.d = L->d;
+        p.n = L->n;
+        for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < L->d ? L->lim[k] : 0;
+        for (s = 0; s < SG_MAX_LEVELS; s++) {
+            if (s < L->n) {
+                sg_layout_eval_shape(L, s, &sh);
+                sg_layout_eval_sub(L, s, &sub);
+                p.blk3[s] = sh.coff[sh.cmax + 1];
+                p.blk2[s] = sub.aoff[sub.amax + 1];
+            } else {
+                p.blk3[s] = p.blk2[s] = 0;
+            }
+        }
+        p.ppt = b->ppt;
+        sgk_fill_eval_args(&p, coords + coff, NULL, out + pt_off[g], pt_off[g + 1] - pt_off[g], &b->h_eval_args[g]);
+        coff += (pt_off[g + 1] - pt_off[g]) * L->d;
+    }
+    /* items grouped by dimension */
+    for (k = 1; k <= SG_MAX_DIMS; k++) {
+        b->items_first[k] = (int)ni;
+        for (g = 0; g < b->ng; g++) {
+            int64_t st;
+            if (b->L[g].d != k) continue;
+            for (st = pt_off[g]; st < pt_off[g + 1]; st += cta) {
+                b->h_items[2 * ni] = g;
+                b->h_items[2 * ni + 1] = (int32_t)(st - pt_off[g]);
+                ni++;
+            }
+        }
+        b->items_count[k] = (int)ni - b->items_first[k];
+    }
+    if (ni > b->items_cap) {
+        cudaFree(b->d_items);
+        b->d_items = NULL;
+        if ((r = balloc(b, (void **)&b->d_items, ni * 2 * 4, "batch eval items")) != SG_OK) return r;
+        b->items_cap = ni;
+    }
+    BCU(cudaMemcpy(b->d_eval_args, b->h_eval_args, (size_t)b->ng * sizeof(sg_eval_args), cudaMemcpyHostToDevice),
+        "upload eval args");
+    if (ni > 0) BCU(cudaMemcpy(b->d_items, b->h_items, (size_t)ni * 2 * 4, cudaMemcpyHostToDevice), "upload items");
+    for (g = 0; g <= b->ng; g++) b->eval_pt_off[g] = pt_off[g];
+    b->eval_coords = coords;
+    b->eval_out = out;
+    b->eval_ppt = b->ppt;
+    return SG_OK;
+}
+
+static int eval_launches(sg_batch *b, cudaStream_t st)
+{
+    int k, e;
+    if ((e = sgk_repack(b->d_alpha, b->d_blk, b->d_repack, b->nrepack, st)) != cudaSuccess)
+        return bcuda((cudaError_t)e, "batch repack");
+    for (k = 1; k <= SG_MAX_DIMS; k++) {
+        if (!b->items_count[k]) continue;
+        e = sgk_evaluate_batch(k, b->d_eval_args, b->d_items + 2 * (int64_t)b->items_first[k], b->items_count[k], b->ppt,
+                               st);
+        if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch evaluate");
+    }
+    return SG_OK;
+}
+
+SG_API int sg_batch_evaluate_device(sg_batch *b, const int64_t *point_offsets, const float *coords, float *out,
+                                    void *stream)
+{
+    int prev, r;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (!b || !point_offsets || point_offsets[0] != 0) return bfail(SG_ERR_ARG, "sg_batch_evaluate_device: bad argument");
+    if (!b->has_values) return bfail(SG_ERR_STATE, "sg_batch_evaluate: no values have been set");
+    if (point_offsets[b->ng] > 0 && (!coords || !out)) return bfail(SG_ERR_ARG, "sg_batch_evaluate_device: NULL buffer");
+    if (point_offsets[b->ng] >= ((int64_t)1 << 31)) return bfail(SG_ERR_RANGE, "sg_batch_evaluate: too many points");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    if ((r = plan_eval(b, point_offsets, coords, out)) == SG_OK)
+        r = b->use_graph ? run_graph(&b->eval_graph, eval_launches, b, st) : eval_launches(b, st);
+    if (r == SG_OK) b->eval_dirty = 0;
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_set_option(sg_batch *b, int option, int64_t value)
+{
+    if (!b) return bfail(SG_ERR_ARG, "sg_batch_set_option: NULL batch");
+    switch (option) {
+    case SG_OPT_HIER_PRECISION:
+        if (value != SG_HIER_FP32 && value != SG_HIER_FP64) return bfail(SG_ERR_ARG, "bad precision");
+        if (b->precision != (int)value && b->hier_graph) {
+            cudaGraphExecDestroy(b->hier_graph);
+            b->hier_graph = NULL;
+        }
+        b->precision = (int)value;
+        return SG_OK;
+    case SG_OPT_EVAL_PPT:
+        if (value < 0 || value > 2) return bfail(SG_ERR_ARG, "SG_OPT_EVAL_PPT is 0, 1 or 2");
+        b->ppt = value == 0 ? 2 : (int)value;
+        return SG_OK;
+    case SG_OPT_USE_GRAPH:
+        if (value != 0 && value != 1) return bfail(SG_ERR_ARG, "SG_OPT_USE_GRAPH is 0 or 1");
+        b->use_graph = (int)value;
+        return SG_OK;
+    default:
+        return bfail(SG_ERR_ARG, "option %d does not apply to batches", option);
+    }
+}
+
+SG_API int sg_batch_device_bytes(const sg_batch *b, int64_t *bytes)
+{
+    if (!b || !bytes) return bfail(SG_ERR_ARG, "sg_batch_device_bytes: NULL argument");
+    *bytes = b->dev_bytes;
+    return SG_OK;
+}

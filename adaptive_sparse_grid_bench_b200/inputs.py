@@ -115,3 +115,39 @@ def grid_values(grid, fn, subspaces=None, chunk: int = 1 << 22) -> np.ndarray:
     for s in range(0, X.shape[0], chunk):
         out[s:s + chunk] = fn(X[s:s + chunk]).astype(np.float32)
     return out
+
+
+def regular_grid_size(d: int, n: int) -> tuple[int, int]:
+    """(points, subspaces) of the regular grid: sum over level sums s < n of
+    C(s+d-1, d-1) subspaces of 2^s points."""
+    from math import comb
+    pts = sum(comb(s + d - 1, d - 1) << s for s in range(n))
+    return pts, comb(n - 1 + d, d)
+
+
+def batch_workload(seed: int, num_grids: int, max_points: int = 2_000_000, d_range=(2, 12), n_range=(3, 9),
+                   pts_range=(256, 65536)):
+    """The batched workload: per grid d and n uniform in the ranges,
+    resampled until the grid has <= max_points points; coefficients
+    (a_k, b_k, c_k) ~ U(-1,1) of f = prod_k (a_k + b_k x_k + c_k x_k^2); a
+    log-uniform number of query points.  Returns dims, levels, coefficient
+    array (num_grids, 3*max_d) and query counts."""
+    dims, levels, counts = [], [], []
+    coef = np.zeros((num_grids, 3 * d_range[1]), np.float64)
+    draw = 0
+    for g in range(num_grids):
+        while True:
+            u = uniform01(seed, 2, start=draw).astype(np.float64)
+            draw += 2
+            d = d_range[0] + int(u[0] * (d_range[1] - d_range[0] + 1))
+            n = n_range[0] + int(u[1] * (n_range[1] - n_range[0] + 1))
+            if regular_grid_size(d, n)[0] <= max_points:
+                break
+        c = uniform01(seed + 1000, 3 * d, start=3 * d_range[1] * g).astype(np.float64) * 2 - 1
+        coef[g, :3 * d] = c
+        lu = uniform01(seed + 2000, 1, start=g).astype(np.float64)[0]
+        m = int(round(np.exp(np.log(pts_range[0]) + lu * (np.log(pts_range[1]) - np.log(pts_range[0])))))
+        dims.append(d)
+        levels.append(n)
+        counts.append(m)
+    return np.array(dims, np.int32), np.array(levels, np.int32), coef, np.array(counts, np.int64)

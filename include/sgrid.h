@@ -64,6 +64,7 @@ extern "C" {
 #define SG_OPT_EVAL_BLOCKS 4    /* subspace blocking: number of passes, 0 = auto     */
 #define SG_OPT_HIER_KERNEL 5    /* 0 = auto, 1 = shared-memory chains, 2 = gather    */
 #define SG_OPT_PROFILE 6        /* 1: record CUDA events around each phase            */
+#define SG_OPT_USE_GRAPH 7      /* batches: 1 (default) capture launches in a CUDA graph */
 
 /* Phases reported by sg_timings (milliseconds of the most recent call). */
 #define SG_PHASE_HIERARCHIZE 0  /* all sweeps of the last hierarchization    */
@@ -158,6 +159,40 @@ int sg_gp2idx_device(const sg_grid *grid, const int *levels, const int *indices,
 /* Fills the grid with f at its points, on the device (replaces the value
  * array like sg_set_values). */
 int sg_sample_function(sg_grid *grid, int fn, const double *params, int num_params, void *stream);
+
+/* ---- batches of independent grids -------------------------------------
+ * Many grids of mixed d, n and limits held in one device buffer and run
+ * through a fixed set of launches (replayed as one CUDA graph).  No
+ * reference counterpart: the reference handles one grid per process.
+ * Values cross the ABI as the grids' compact arrays concatenated in grid
+ * order (offsets from sg_batch_offsets).  limits: NULL, or every grid's d
+ * limits concatenated. */
+typedef struct sg_batch sg_batch;
+int sg_batch_create(int num_grids, const int *dims, const int *levels, const int *limits,
+                    sg_batch **batch);
+int sg_batch_destroy(sg_batch *batch);
+int sg_batch_num_grids(const sg_batch *batch, int *num_grids);
+/* value_offsets[num_grids+1]: first value of each grid in the concatenation */
+int sg_batch_offsets(const sg_batch *batch, int64_t *value_offsets);
+int sg_batch_set_values(sg_batch *batch, const float *values);
+int sg_batch_set_values_device(sg_batch *batch, const float *values, void *stream);
+int sg_batch_get_values(sg_batch *batch, float *values);
+/* params: params_per_grid doubles per grid (SG_FN_QUAD: 3*d of them) */
+int sg_batch_sample_function(sg_batch *batch, int fn, const double *params, int params_per_grid,
+                             void *stream);
+/* All grids, one graph launch; bit-identical to sg_hierarchize per grid. */
+int sg_batch_hierarchize_async(sg_batch *batch, void *stream);
+int sg_batch_hierarchize(sg_batch *batch);
+/* Grid g is evaluated at the point_offsets[g+1]-point_offsets[g] points
+ * whose coordinates follow each other in `coord_mat` (rows of d_g floats,
+ * grid after grid); results land at out[point_offsets[g] ...].  Device
+ * pointers; point_offsets is a host array of num_grids+1 entries. */
+int sg_batch_evaluate_device(sg_batch *batch, const int64_t *point_offsets, const float *coord_mat,
+                             float *out, void *stream);
+int sg_batch_sync(sg_batch *batch, void *stream);
+/* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH */
+int sg_batch_set_option(sg_batch *batch, int option, int64_t value);
+int sg_batch_device_bytes(const sg_batch *batch, int64_t *bytes);
 
 /* ---- options and diagnostics ------------------------------------------ */
 int sg_set_option(sg_grid *grid, int option, int64_t value);

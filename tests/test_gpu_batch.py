@@ -1,0 +1,96 @@
+"""Batches of grids on the GPU: bit-identical hierarchization to the
+single-grid path (and hence to hierarchize0), evaluation equal to the
+single-grid evaluation, in both precisions, with and without CUDA graphs."""
+import numpy as np
+import pytest
+
+import adaptive_sparse_grid_bench_b200 as sg
+from adaptive_sparse_grid_bench_b200 import _lib, inputs
+
+pytestmark = pytest.mark.gpu
+
+MIXED = [  # (d, n, limits): small grids (shared-memory path) and larger ones (sweeps)
+    (2, 3, None), (4, 8, None), (3, 7, [6, 2, 4]), (6, 6, None), (10, 5, None), (1, 9, None),
+    (12, 4, None), (5, 9, None), (3, 12, None), (8, 7, None), (2, 9, [8, 3]), (4, 9, None)]
+
+
+def _batch(shapes):
+    dims = [s[0] for s in shapes]
+    levels = [s[1] for s in shapes]
+    limits = None
+    if any(s[2] is not None for s in shapes):
+        limits = [s[2] if s[2] is not None else [s[1] - 1] * s[0] for s in shapes]
+    return sg.Batch(dims, levels, limits)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+@pytest.mark.parametrize("graph", [1, 0])
+def test_batch_hierarchize_matches_single_grids(cuda, precision, graph):
+    b = _batch(MIXED)
+    b.set_option(_lib.SG_OPT_USE_GRAPH, graph)
+    b.set_option(_lib.SG_OPT_HIER_PRECISION, _lib.SG_HIER_FP64 if precision == "fp64" else _lib.SG_HIER_FP32)
+    vals = inputs.uniform01(77, b.num_values) * 2 - 1
+    for rep in range(2):  # the second run replays the graph
+        b.set_values(vals)
+        b.hierarchize()
+        got = b.get_values()
+    for g, (d, n, lim) in enumerate(MIXED):
+        one = sg.Grid(d, n, lim)
+        one.precision = precision
+        one.set_values(b.grid_values(vals, g))
+        one.hierarchize()
+        want = one.get_values()
+        assert np.array_equal(b.grid_values(got, g).view(np.uint32), want.view(np.uint32)), f"grid {g} {d} {n}"
+
+
+@pytest.mark.parametrize("ppt", [1, 2])
+def test_batch_evaluate_matches_single_grids(cuda, ppt):
+    import torch
+    b = _batch(MIXED)
+    b.set_option(_lib.SG_OPT_EVAL_PPT, ppt)
+    vals = inputs.uniform01(78, b.num_values) * 2 - 1
+    b.set_values(vals)
+    b.hierarchize()
+    counts = [0, 1, 513, 1000, 257, 33, 2048, 600, 70, 511, 512, 1025]
+    po = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    Xs = [inputs.uniform_points(100 + g, counts[g], MIXED[g][0]) for g in range(len(MIXED))]
+    coords = torch.from_numpy(np.concatenate([x.reshape(-1) for x in Xs]).astype(np.float32)).to(cuda)
+    out = torch.full((int(po[-1]),), np.nan, device=cuda)
+    for rep in range(2):
+        b.evaluate_device(po, coords, out)
+        b.sync()
+    res = out.cpu().numpy()
+    surplus = b.get_values()
+    for g, (d, n, lim) in enumerate(MIXED):
+        if counts[g] == 0:
+            continue
+        one = sg.Grid(d, n, lim)
+        one.set_values(b.grid_values(surplus, g))
+        want = one.evaluate(Xs[g])
+        got = res[po[g]:po[g + 1]]
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"grid {g}"
+
+
+def test_batch_sample_quad_and_config_like_workload(cuda):
+    import torch
+    dims, levels, coef, counts = inputs.batch_workload(3, 64, max_points=200_000)
+    b = sg.Batch(dims, levels)
+    b.sample_function(_lib.SG_FN_QUAD, coef)
+    b.hierarchize()
+    surplus = b.get_values()
+    po = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    Xs = [inputs.uniform_points(200 + g, int(counts[g]), int(dims[g])) for g in range(len(dims))]
+    coords = torch.from_numpy(np.concatenate([x.reshape(-1) for x in Xs])).to(cuda)
+    out = torch.empty(int(po[-1]), device=cuda)
+    b.evaluate_device(po, coords, out)
+    b.sync()
+    res = out.cpu().numpy()
+    for g in range(0, len(dims), 9):
+        one = sg.Grid(int(dims[g]), int(levels[g]))
+        one.sample_function(_lib.SG_FN_QUAD, coef[g, :3 * dims[g]])
+        vals = one.get_values()
+        one.hierarchize()
+        assert np.array_equal(one.get_values().view(np.uint32), b.grid_values(surplus, g).view(np.uint32))
+        want = one.evaluate(Xs[g])
+        assert np.array_equal(res[po[g]:po[g + 1]].view(np.uint32), want.view(np.uint32))
+        assert vals.size == b.grid_values(surplus, g).size
