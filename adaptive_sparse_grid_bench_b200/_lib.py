@@ -87,6 +87,7 @@ SIGNATURES = {
     "sg_batch_set_values": (_i, [_p, _p]),
     "sg_batch_set_values_device": (_i, [_p, _p, _p]),
     "sg_batch_get_values": (_i, [_p, _p]),
+    "sg_batch_get_values_device": (_i, [_p, _p, _p]),
     "sg_batch_sample_function": (_i, [_p, _i, _p, _i, _p]),
     "sg_batch_hierarchize_async": (_i, [_p, _p]),
     "sg_batch_hierarchize": (_i, [_p]),

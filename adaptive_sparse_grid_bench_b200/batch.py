@@ -67,6 +67,9 @@ class Batch:
         check(L.lib().sg_batch_get_values(self._h, out.ctypes.data))
         return out
 
+    def get_values_device(self, values, stream=None) -> None:
+        check(L.lib().sg_batch_get_values_device(self._h, int(values.data_ptr()), _stream_handle(stream)))
+
     def grid_values(self, all_values, g: int) -> np.ndarray:
         return all_values[self.value_offsets[g]:self.value_offsets[g + 1]]
 

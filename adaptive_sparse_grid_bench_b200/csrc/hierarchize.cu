@@ -371,6 +371,20 @@ __global__ void k_narrow(const double *__restrict__ s, float *__restrict__ d, in
         d[i] = __double2float_rn(s[i]);
 }
 
+/* dst[seg.dst + i] = src[seg.src + i] for i < seg.count, one segment per
+ * CTA iteration (moves values between the caller's compact concatenation
+ * and a batch's group-aligned layout in one launch). */
+__global__ void k_copy_segments(const float *__restrict__ src, float *__restrict__ dst,
+                                const sg_copy_seg *__restrict__ segs, int64_t nseg, int to_compact)
+{
+    for (int64_t q = blockIdx.x; q < nseg; q += gridDim.x) {
+        const sg_copy_seg sgm = segs[q];
+        const int64_t from = to_compact ? sgm.dev : sgm.compact;
+        const int64_t to = to_compact ? sgm.compact : sgm.dev;
+        for (int64_t i = threadIdx.x; i < sgm.count; i += blockDim.x) dst[to + i] = src[from + i];
+    }
+}
+
 int g_num_sms = 0;
 long long g_launches = 0;
 
@@ -475,6 +489,16 @@ int sgk_widen(const float *src, double *dst, int64_t n, void *stream)
     int64_t g = (n + 255) / 256;
     if (g > 148 * 32) g = 148 * 32;
     k_widen<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(src, dst, n);
+    sgk_count(1);
+    return cudaGetLastError();
+}
+
+int sgk_copy_segments(const float *src, float *dst, const sg_copy_seg *segs, int64_t nseg, int to_compact,
+                      void *stream)
+{
+    if (nseg <= 0) return cudaSuccess;
+    int64_t g = nseg < 148 * 32 ? nseg : 148 * 32;
+    k_copy_segments<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(src, dst, segs, nseg, to_compact);
     sgk_count(1);
     return cudaGetLastError();
 }

@@ -24,6 +24,9 @@ struct sg_batch {
     double *d_work;      /* FP64 sweep values (lazy)                              */
     float *d_blk;        /* all grids, block layout                               */
     int *d_err;
+    sg_copy_seg *d_segs;  /* per-grid level groups: compact <-> device layout */
+    int64_t nsegs;
+    float *d_stage;       /* host-buffer transfers: compact values on the device (lazy) */
     /* shared-memory path */
     int n_smem;
     int cls_first[SG_BATCH_CLASSES], cls_count[SG_BATCH_CLASSES], cls_max_npad[SG_BATCH_CLASSES];

@@ -36,6 +36,14 @@ int sgk_sweep_chains_f64(double *a, const sg_sweep_tables *t, int *err, void *st
 int sgk_sweep_gather_f32(float *a, const sg_sweep_tables *t, void *stream);
 int sgk_sweep_gather_f64(double *a, const sg_sweep_tables *t, void *stream);
 int sgk_widen(const float *src, double *dst, int64_t n, void *stream);
+
+/* A run of values at `compact` in a caller's compact array and at `dev` in
+ * a device layout. */
+typedef struct sg_copy_seg {
+    int64_t compact, dev, count;
+} sg_copy_seg;
+int sgk_copy_segments(const float *src, float *dst, const sg_copy_seg *segs, int64_t nseg, int to_compact,
+                      void *stream);
 int sgk_narrow(const double *src, float *dst, int64_t n, void *stream);
 
 /* Evaluation. */

@@ -116,6 +116,8 @@ static void free_dev(sg_batch *b)
     cudaFree(b->d_eval_args);
     cudaFree(b->d_items);
     cudaFree(b->d_err);
+    cudaFree(b->d_segs);
+    cudaFree(b->d_stage);
     free(b->h_eval_args);
     free(b->h_items);
     b->h_eval_args = NULL;
@@ -216,6 +218,31 @@ static int materialize(sg_batch *b)
     if ((r = balloc(b, (void **)&b->d_blk, b->boff[b->ng] * 4, "batch block layout")) != SG_OK) goto done;
     if ((r = balloc(b, (void **)&b->d_err, 16, "error flag")) != SG_OK) goto done;
     BCU(cudaMemset(b->d_err, 0, 16), "cudaMemset");
+
+    /* level-group runs for moving values in one launch */
+    {
+        int64_t ns = 0;
+        sg_copy_seg *segs;
+        for (g = 0; g < b->ng; g++) ns += b->L[g].n;
+        segs = (sg_copy_seg *)malloc((size_t)ns * sizeof(sg_copy_seg));
+        if (!segs) { r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
+        ns = 0;
+        for (g = 0; g < b->ng; g++) {
+            int s;
+            const sg_layout *L = &b->L[g];
+            for (s = 0; s < L->n; s++) {
+                if (L->lidx[s + 1] == L->lidx[s]) continue;
+                segs[ns].compact = b->voff[g] + L->lidx[s];
+                segs[ns].dev = b->doff[g] + L->plidx[s];
+                segs[ns].count = L->lidx[s + 1] - L->lidx[s];
+                ns++;
+            }
+        }
+        b->nsegs = ns;
+        r = upload(b, (void **)&b->d_segs, segs, ns * (int64_t)sizeof(sg_copy_seg), "batch value runs");
+        free(segs);
+        if (r != SG_OK) goto done;
+    }
 
     /* shared-memory path: grids in size classes, largest first inside each */
     order = (int *)malloc((size_t)b->ng * sizeof(int));
@@ -369,21 +396,16 @@ static void leave(sg_batch *b, int prev)
     if (b->dev >= 0 && b->dev != prev) cudaSetDevice(prev);
 }
 
-static int copy_values(sg_batch *b, float *dst, const float *src, int to_dev, enum cudaMemcpyKind kind, cudaStream_t st)
+/* compact concatenation (device) <-> group-aligned batch layout, one launch */
+static int move_values(sg_batch *b, const float *src, float *dst, int to_compact, cudaStream_t st)
 {
-    int g, s;
-    for (g = 0; g < b->ng; g++) {
-        const sg_layout *L = &b->L[g];
-        for (s = 0; s < L->n; s++) {
-            const int64_t cnt = L->lidx[s + 1] - L->lidx[s];
-            const int64_t c_off = b->voff[g] + L->lidx[s], d_off = b->doff[g] + L->plidx[s];
-            if (cnt == 0) continue;
-            BCU(cudaMemcpyAsync(to_dev ? dst + d_off : dst + c_off, to_dev ? src + c_off : src + d_off,
-                                (size_t)cnt * 4, kind, st),
-                "batch value copy");
-        }
-    }
-    return SG_OK;
+    int e = sgk_copy_segments(src, dst, b->d_segs, b->nsegs, to_compact, st);
+    return e == cudaSuccess ? SG_OK : bcuda((cudaError_t)e, "batch value move");
+}
+
+static int ensure_stage(sg_batch *b)
+{
+    return b->d_stage ? SG_OK : balloc(b, (void **)&b->d_stage, b->voff[b->ng] * 4, "batch transfer staging");
 }
 
 SG_API int sg_batch_set_values(sg_batch *b, const float *values)
@@ -391,10 +413,14 @@ SG_API int sg_batch_set_values(sg_batch *b, const float *values)
     int prev, r;
     if (!b || !values) return bfail(SG_ERR_ARG, "sg_batch_set_values: NULL argument");
     if ((r = enter(b, &prev)) != SG_OK) return r;
-    if ((r = materialize(b)) == SG_OK && (r = copy_values(b, b->d_alpha, values, 1, cudaMemcpyHostToDevice, 0)) == SG_OK) {
-        cudaError_t e = cudaStreamSynchronize(0);
+    if ((r = materialize(b)) == SG_OK && (r = ensure_stage(b)) == SG_OK) {
+        cudaError_t e = cudaMemcpy(b->d_stage, values, (size_t)b->voff[b->ng] * 4, cudaMemcpyHostToDevice);
         if (e != cudaSuccess) r = bcuda(e, "sg_batch_set_values");
-        else b->has_values = 1, b->eval_dirty = 1;
+        else if ((r = move_values(b, b->d_stage, b->d_alpha, 0, 0)) == SG_OK) {
+            e = cudaStreamSynchronize(0);
+            if (e != cudaSuccess) r = bcuda(e, "sg_batch_set_values");
+            else b->has_values = 1, b->eval_dirty = 1;
+        }
     }
     leave(b, prev);
     return r;
@@ -405,8 +431,7 @@ SG_API int sg_batch_set_values_device(sg_batch *b, const float *values, void *st
     int prev, r;
     if (!b || !values) return bfail(SG_ERR_ARG, "sg_batch_set_values_device: NULL argument");
     if ((r = enter(b, &prev)) != SG_OK) return r;
-    if ((r = materialize(b)) == SG_OK &&
-        (r = copy_values(b, b->d_alpha, values, 1, cudaMemcpyDeviceToDevice, (cudaStream_t)stream)) == SG_OK)
+    if ((r = materialize(b)) == SG_OK && (r = move_values(b, values, b->d_alpha, 0, (cudaStream_t)stream)) == SG_OK)
         b->has_values = 1, b->eval_dirty = 1;
     leave(b, prev);
     return r;
@@ -418,10 +443,21 @@ SG_API int sg_batch_get_values(sg_batch *b, float *values)
     if (!b || !values) return bfail(SG_ERR_ARG, "sg_batch_get_values: NULL argument");
     if (!b->has_values) return bfail(SG_ERR_STATE, "sg_batch_get_values: no values have been set");
     if ((r = enter(b, &prev)) != SG_OK) return r;
-    if ((r = copy_values(b, values, b->d_alpha, 0, cudaMemcpyDeviceToHost, 0)) == SG_OK) {
-        cudaError_t e = cudaStreamSynchronize(0);
+    if ((r = ensure_stage(b)) == SG_OK && (r = move_values(b, b->d_alpha, b->d_stage, 1, 0)) == SG_OK) {
+        cudaError_t e = cudaMemcpy(values, b->d_stage, (size_t)b->voff[b->ng] * 4, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess) r = bcuda(e, "sg_batch_get_values");
     }
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_get_values_device(sg_batch *b, float *values, void *stream)
+{
+    int prev, r;
+    if (!b || !values) return bfail(SG_ERR_ARG, "sg_batch_get_values_device: NULL argument");
+    if (!b->has_values) return bfail(SG_ERR_STATE, "sg_batch_get_values_device: no values have been set");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    r = move_values(b, b->d_alpha, values, 1, (cudaStream_t)stream);
     leave(b, prev);
     return r;
 }

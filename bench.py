@@ -48,6 +48,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per reference sample")
+    ap.add_argument("--workload", default="single", choices=["single", "batched"],
+                    help="single: the d=10 n=10 grid (default); batched: many grids of mixed d and n")
+    ap.add_argument("--grids", type=int, default=4096, help="batched: number of grids")
     return ap.parse_args()
 
 
@@ -317,6 +320,115 @@ def run_b200(args, rank: int, world: int, local_rank: int):
     print(json.dumps(line), flush=True)
 
 
+def run_batched(args, rank: int, world: int, local_rank: int):
+    """Batched workload: `--grids` grids with d uniform in 2..12 and n in
+    3..9 (at most 2e6 points each), f = prod_k (a_k + b_k x + c_k x^2) with
+    coefficients ~U(-1,1) (seed 3), each evaluated at a log-uniform
+    256..65536 uniform points.  One step = restore nodal values, hierarchize
+    every grid (one graph launch), evaluate every grid (one graph launch).
+    Also timed: the same grids one plain launch sequence per grid (a sample
+    of grids), the reference's arrangement of one grid per run."""
+    import torch
+    from adaptive_sparse_grid_bench_b200 import Batch, Grid, inputs
+    from adaptive_sparse_grid_bench_b200._lib import (SG_FN_QUAD, SG_HIER_FP32, SG_HIER_FP64, SG_OPT_HIER_PRECISION,
+                                                      kernel_launches)
+    from adaptive_sparse_grid_bench_b200.sharding import max_over_ranks
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    dims, levels, coef, counts = inputs.batch_workload(3 + rank, args.grids)
+    b = Batch(dims, levels)
+    b.set_option(SG_OPT_HIER_PRECISION, SG_HIER_FP64 if args.precision == "fp64" else SG_HIER_FP32)
+    b.sample_function(SG_FN_QUAD, coef)
+    vals = torch.empty(b.num_values, dtype=torch.float32, device=dev)
+    b.get_values_device(vals)
+    po = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    nflt = int(np.sum(counts * dims))
+    X = torch.from_numpy(inputs.uniform01(SEED + 100 + rank, nflt)).to(dev)
+    out = torch.empty(int(po[-1]), dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream()
+    npts = [inputs.regular_grid_size(int(d), int(n))[0] for d, n in zip(dims, levels)]
+
+    def step():
+        b.set_values_device(vals, stream)
+        b.hierarchize_async(stream)
+        b.evaluate_device(po, X, out, stream)
+
+    for _ in range(args.warmup):
+        step()
+    b.sync(stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    th, te = [], []
+    with Clocks(local_rank) as clk:
+        torch.cuda.synchronize()
+        l0 = kernel_launches()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            b.set_values_device(vals, stream)
+            ev[0].record(stream)
+            b.hierarchize_async(stream)
+            ev[1].record(stream)
+            b.evaluate_device(po, X, out, stream)
+            ev[2].record(stream)
+            ev[2].synchronize()
+            th.append(ev[0].elapsed_time(ev[1]))
+            te.append(ev[1].elapsed_time(ev[2]))
+        e1.record(stream)
+        torch.cuda.synchronize()
+        launches = kernel_launches() - l0
+    b.sync(stream)
+    ms = e0.elapsed_time(e1)
+    ms_max = max_over_ranks(ms, dev) if world > 1 else ms
+    total_pts = int(po[-1])
+    value = world * total_pts * args.steps / (ms_max / 1e3)
+
+    # one plain launch sequence per grid (sample of grids, extrapolated)
+    sample = list(range(0, len(dims), max(1, len(dims) // 128)))
+    plain_pts, plain_ms = 0, 0.0
+    xs = X.cpu().numpy()
+    coff = np.concatenate([[0], np.cumsum(counts * dims)])
+    for g in sample:
+        one = Grid(int(dims[g]), int(levels[g]))
+        one.sample_function(SG_FN_QUAD, coef[g, :3 * dims[g]])
+        nod = torch.empty(one.num_points, device=dev)
+        one.get_values_device(nod)
+        xg = torch.from_numpy(xs[coff[g]:coff[g + 1]].copy()).to(dev)
+        og = torch.empty(int(counts[g]), device=dev)
+        for rep in range(2):
+            s0 = torch.cuda.Event(enable_timing=True)
+            s1 = torch.cuda.Event(enable_timing=True)
+            s0.record(stream)
+            one.set_values_device(nod, stream)
+            one.hierarchize_async(stream)
+            one.evaluate_device(xg, og, int(counts[g]), stream)
+            s1.record(stream)
+            s1.synchronize()
+        plain_ms += s0.elapsed_time(s1)
+        plain_pts += int(counts[g])
+        one.close()
+    plain_value = plain_pts / (plain_ms / 1e3)
+    if rank != 0:
+        return
+    hier_bytes = 8.0 * float(np.sum(np.array(npts) * dims))
+    line = {
+        "metric": "evals/s (batched grids)", "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)",
+        "config": {"workload": f"{len(dims)} grids, d in 2..12, n in 3..9, <= 2e6 points each, f = prod(a+bx+cx^2),"
+                               f" 256..65536 log-uniform points per grid", "grids": len(dims),
+                   "grid_points": int(sum(npts)), "query_points": total_pts, "hier_precision": args.precision},
+        "hierarchize": {"ms": statistics.mean(th), "GB/s_8dN": hier_bytes / (statistics.mean(th) / 1e3) / 1e9,
+                        "grids_per_s": len(dims) / (statistics.mean(th) / 1e3)},
+        "evaluate": {"ms": statistics.mean(te), "evals_per_s": total_pts / (statistics.mean(te) / 1e3)},
+        "plain_per_grid": {"evals_per_s": plain_value, "grids_sampled": len(sample),
+                           "note": "one set_values/hierarchize/evaluate launch sequence per grid, summed"},
+        "speedup_vs_plain": value / plain_value,
+        "gpu_launches": int(launches), "clocks": clk.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -333,7 +445,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     try:
-        run_b200(args, rank, world, local_rank)
+        if args.workload == "batched":
+            run_batched(args, rank, world, local_rank)
+        else:
+            run_b200(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -177,6 +177,7 @@ int sg_batch_offsets(const sg_batch *batch, int64_t *value_offsets);
 int sg_batch_set_values(sg_batch *batch, const float *values);
 int sg_batch_set_values_device(sg_batch *batch, const float *values, void *stream);
 int sg_batch_get_values(sg_batch *batch, float *values);
+int sg_batch_get_values_device(sg_batch *batch, float *values, void *stream);
 /* params: params_per_grid doubles per grid (SG_FN_QUAD: 3*d of them) */
 int sg_batch_sample_function(sg_batch *batch, int fn, const double *params, int params_per_grid,
                              void *stream);
