@@ -95,6 +95,13 @@ SIGNATURES = {
     "sg_batch_sync": (_i, [_p, _p]),
     "sg_batch_set_option": (_i, [_p, _i, _i64]),
     "sg_batch_device_bytes": (_i, [_p, _pi64]),
+    "sg_server_create": (_i, [_i64, _i64, C.POINTER(_p)]),
+    "sg_server_destroy": (_i, [_p]),
+    "sg_server_add_grid": (_i, [_p, _i, _i, _p, _i, _p, _i, _pi64]),
+    "sg_server_submit": (_i, [_p, _i64, _p, _i64, _p, _pi64]),
+    "sg_server_wait": (_i, [_p, _i64, C.POINTER(C.c_double)]),
+    "sg_server_stats": (_i, [_p, _p]),
+    "sg_server_evaluate_now": (_i, [_p, _i64, _p, _i64, _p]),
     "sg_last_error": (C.c_char_p, []),
     "sg_version": (C.c_char_p, []),
 }

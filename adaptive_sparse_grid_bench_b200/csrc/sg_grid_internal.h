@@ -1,0 +1,45 @@
+/* Internal state of a single-grid handle (sgrid.c), shared with the
+ * serving loop (sgrid_server.c). */
+#ifndef SG_GRID_INTERNAL_H
+#define SG_GRID_INTERNAL_H
+
+#include <cuda_runtime_api.h>
+#include <stdint.h>
+
+#include "sg_kernels.h"
+#include "sg_layout.h"
+
+#define NOPT 8
+
+struct sg_grid {
+    sg_layout L;
+    int dev;        /* device of the device state, -1 before it exists */
+    int has_values; /* a value array has been stored                   */
+    int64_t opt[NOPT];
+    float *d_alpha;   /* Npad floats, group-aligned layout         */
+    double *d_work;   /* Npad doubles, FP64 hierarchization (lazy) */
+    float *d_blk;        /* N floats: surpluses in the block layout    */
+    sg_repack *d_repack; /* per-subspace compact -> block descriptors  */
+    uint32_t blk3[SG_MAX_LEVELS]; /* block size per level budget        */
+    uint32_t blk2[SG_MAX_LEVELS]; /* sub-block size per level budget    */
+    int eval_dirty;      /* d_blk is stale                              */
+    sg_chain *d_chains[SG_MAX_DIMS];
+    uint32_t *d_seg[SG_MAX_DIMS];
+    sg_sweep_tables sweep[SG_MAX_DIMS];
+    int *d_err;       /* device-side wait timeout flag             */
+    void *d_scratch;  /* evaluate: sort scratch + sorted coords + permutation */
+    int64_t scratch_bytes;
+    void *d_io;       /* host-buffer evaluate: staged coords and results */
+    int64_t io_bytes;
+    int64_t dev_bytes;
+    cudaEvent_t ev[SG_NUM_PHASES][2]; /* profiling: start/stop per phase */
+    int ev_used[SG_NUM_PHASES];
+};
+
+
+/* Builds the block layout if the values changed since it was last built. */
+int sg_grid_prepare_eval(sg_grid *g, cudaStream_t st);
+/* Kernel arguments to evaluate grid g at m points (device pointers). */
+void sg_grid_eval_args(const sg_grid *g, const float *coords, float *out, int64_t m, sg_eval_args *a);
+
+#endif

@@ -13,37 +13,11 @@
 
 #include "sg_kernels.h"
 #include "sg_batch_internal.h"
+#include "sg_grid_internal.h"
 #include "sg_layout.h"
 
 #define SG_API __attribute__((visibility("default")))
 #define SG_VERSION "sgb200 0.1.0"
-
-#define NOPT 8
-
-struct sg_grid {
-    sg_layout L;
-    int dev;        /* device of the device state, -1 before it exists */
-    int has_values; /* a value array has been stored                   */
-    int64_t opt[NOPT];
-    float *d_alpha;   /* Npad floats, group-aligned layout         */
-    double *d_work;   /* Npad doubles, FP64 hierarchization (lazy) */
-    float *d_blk;        /* N floats: surpluses in the block layout    */
-    sg_repack *d_repack; /* per-subspace compact -> block descriptors  */
-    uint32_t blk3[SG_MAX_LEVELS]; /* block size per level budget        */
-    uint32_t blk2[SG_MAX_LEVELS]; /* sub-block size per level budget    */
-    int eval_dirty;      /* d_blk is stale                              */
-    sg_chain *d_chains[SG_MAX_DIMS];
-    uint32_t *d_seg[SG_MAX_DIMS];
-    sg_sweep_tables sweep[SG_MAX_DIMS];
-    int *d_err;       /* device-side wait timeout flag             */
-    void *d_scratch;  /* evaluate: sort scratch + sorted coords + permutation */
-    int64_t scratch_bytes;
-    void *d_io;       /* host-buffer evaluate: staged coords and results */
-    int64_t io_bytes;
-    int64_t dev_bytes;
-    cudaEvent_t ev[SG_NUM_PHASES][2]; /* profiling: start/stop per phase */
-    int ev_used[SG_NUM_PHASES];
-};
 
 static __thread char g_err[512];
 
@@ -752,4 +726,32 @@ SG_API int sg_device_bytes(const sg_grid *g, int64_t *bytes)
     if (!g || !bytes) return fail(SG_ERR_ARG, "sg_device_bytes: NULL argument");
     *bytes = g->dev_bytes;
     return SG_OK;
+}
+
+/* ---- internal, for the serving loop ------------------------------------- */
+
+int sg_grid_prepare_eval(sg_grid *g, cudaStream_t st)
+{
+    int e;
+    if (!g->eval_dirty) return SG_OK;
+    if ((e = sgk_repack(g->d_alpha, g->d_blk, g->d_repack, g->L.S, st)) != cudaSuccess)
+        return cuda_fail((cudaError_t)e, "repacking surpluses");
+    g->eval_dirty = 0;
+    return SG_OK;
+}
+
+void sg_grid_eval_args(const sg_grid *g, const float *coords, float *out, int64_t m, sg_eval_args *a)
+{
+    sg_eval_plan p;
+    int k;
+    p.alpha = g->d_blk;
+    p.d = g->L.d;
+    p.n = g->L.n;
+    for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < g->L.d ? g->L.lim[k] : 0;
+    for (k = 0; k < SG_MAX_LEVELS; k++) {
+        p.blk3[k] = g->blk3[k];
+        p.blk2[k] = g->blk2[k];
+    }
+    p.ppt = 2;
+    sgk_fill_eval_args(&p, coords, NULL, out, m, a);
 }

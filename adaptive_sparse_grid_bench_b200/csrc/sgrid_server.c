@@ -1,0 +1,562 @@
+/*
+ * Serving loop (sg_server_* in include/sgrid.h).  Host code in C with one
+ * dispatcher thread.
+ *
+ * Resident grids: a pool of hierarchized grids kept on the device under a
+ * byte cap.  sg_server_add_grid admits a new grid (create, sample,
+ * hierarchize, build the evaluation layout) after evicting least recently
+ * used grids that no queued or running request needs; if that cannot free
+ * enough memory the admission fails with SG_ERR_NOMEM.
+ *
+ * Continuous batching: callers submit evaluate requests of any size (up to
+ * the batch capacity) against resident grids and get a ticket.  The
+ * dispatcher takes every request queued at that moment (up to the capacity)
+ * into one batch: one host->device copy of all their coordinates, one
+ * batched evaluation launch per dimension present (the batched kernel treats
+ * each request as a grid of its own), one device->host copy of the results.
+ * Batches alternate between two slots with their own streams, so a batch is
+ * assembled and copied while the previous one computes; requests that arrive
+ * while a batch runs go into the next one as soon as a slot frees up.  A
+ * request's result depends only on its grid and points, so it is the same
+ * alone and in any mix.
+ */
+#include <cuda_runtime_api.h>
+#include <pthread.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "sg_batch_internal.h"
+#include "sg_grid_internal.h"
+#include "sg_kernels.h"
+
+#define SG_API __attribute__((visibility("default")))
+#define SRV_SLOTS 2
+#define SRV_MAX_REQS 8192 /* requests per batch */
+#define SG_SERVER_CTA_POINTS 512 /* points per CTA of the batched kernel at 2 per thread */
+
+typedef struct srv_grid {
+    int64_t id;
+    sg_grid *g;
+    int64_t bytes;
+    uint64_t last_used;
+    int pins;  /* queued or running requests */
+    int alive;
+} srv_grid;
+
+typedef struct srv_req {
+    int64_t ticket;
+    int gi; /* index in the grid table */
+    int d;
+    const float *coords;
+    float *out;
+    int64_t m;
+    double t_submit, t_done;
+    int state; /* 0 queued, 1 running, 2 done, 3 failed */
+    struct srv_req *next;
+} srv_req;
+
+typedef struct srv_slot {
+    cudaStream_t st;
+    cudaEvent_t done;
+    int busy;
+    float *h_coords, *h_out, *d_coords, *d_out;
+    sg_eval_args *h_args, *d_args;
+    int32_t *h_items, *d_items;
+    srv_req *reqs[SRV_MAX_REQS];
+    int64_t out_off[SRV_MAX_REQS];
+    int nreq;
+} srv_slot;
+
+struct sg_server {
+    int dev;
+    pthread_mutex_t mu;
+    pthread_mutex_t plain_mu; /* serialises sg_server_evaluate_now: a grid handle serves one thread at a time */
+    pthread_cond_t cv_work, cv_done;
+    pthread_t thr;
+    int running, thread_ok;
+    srv_grid *grids;
+    int ngrids, cap_grids;
+    int64_t next_id, cap_bytes, used_bytes;
+    uint64_t clock;
+    srv_req *head, *tail;
+    int64_t queued_points;
+    srv_req **by_ticket;
+    int64_t next_ticket, cap_tickets;
+    int64_t max_points;
+    srv_slot slot[SRV_SLOTS];
+    cudaStream_t admit_st;
+    int64_t st_batches, st_requests, st_points, st_evictions, st_failed;
+    int fatal; /* a CUDA error in the dispatcher: the server is unusable */
+};
+
+static int sfail(int code, const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    sg_set_error(fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+static double now_ms(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
+}
+
+static void finish_slot(sg_server *s, srv_slot *sl, int ok)
+{
+    const double t = now_ms();
+    int i;
+    for (i = 0; i < sl->nreq; i++) {
+        srv_req *r = sl->reqs[i];
+        if (ok) memcpy(r->out, sl->h_out + sl->out_off[i], (size_t)r->m * sizeof(float));
+        r->t_done = t;
+        r->state = ok ? 2 : 3;
+        s->grids[r->gi].pins--;
+        if (!ok) s->st_failed++;
+    }
+    sl->nreq = 0;
+    sl->busy = 0;
+    pthread_cond_broadcast(&s->cv_done);
+}
+
+/* Fills slot sl with queued requests (lock held) and returns their count. */
+static int take_batch(sg_server *s, srv_slot *sl)
+{
+    int64_t pts = 0, coff = 0;
+    sl->nreq = 0;
+    while (s->head && sl->nreq < SRV_MAX_REQS) {
+        srv_req *r = s->head;
+        if (sl->nreq > 0 && pts + r->m > s->max_points) break;
+        s->head = r->next;
+        if (!s->head) s->tail = NULL;
+        s->queued_points -= r->m;
+        r->state = 1;
+        sl->reqs[sl->nreq] = r;
+        sl->out_off[sl->nreq] = pts;
+        memcpy(sl->h_coords + coff, r->coords, (size_t)(r->m * r->d) * sizeof(float));
+        sg_grid_eval_args(s->grids[r->gi].g, sl->d_coords + coff, sl->d_out + pts, r->m, &sl->h_args[sl->nreq]);
+        coff += r->m * r->d;
+        pts += r->m;
+        sl->nreq++;
+    }
+    return sl->nreq;
+}
+
+/* Copies in, one batched evaluation launch per dimension, copies out. */
+static int launch_batch(sg_server *s, srv_slot *sl)
+{
+    int64_t coff = 0, pts = 0, ni = 0;
+    int i, d, e;
+    int first[SG_MAX_DIMS + 1], count[SG_MAX_DIMS + 1];
+    for (i = 0; i < sl->nreq; i++) {
+        coff += sl->reqs[i]->m * sl->reqs[i]->d;
+        pts += sl->reqs[i]->m;
+    }
+    for (d = 1; d <= SG_MAX_DIMS; d++) {
+        first[d] = (int)ni;
+        for (i = 0; i < sl->nreq; i++) {
+            int64_t p;
+            if (sl->reqs[i]->d != d) continue;
+            for (p = 0; p < sl->reqs[i]->m; p += SG_SERVER_CTA_POINTS) {
+                sl->h_items[2 * ni] = i;
+                sl->h_items[2 * ni + 1] = (int32_t)p;
+                ni++;
+            }
+        }
+        count[d] = (int)ni - first[d];
+    }
+    if (cudaMemcpyAsync(sl->d_coords, sl->h_coords, (size_t)coff * 4, cudaMemcpyHostToDevice, sl->st) != cudaSuccess ||
+        cudaMemcpyAsync(sl->d_args, sl->h_args, (size_t)sl->nreq * sizeof(sg_eval_args), cudaMemcpyHostToDevice,
+                        sl->st) != cudaSuccess ||
+        cudaMemcpyAsync(sl->d_items, sl->h_items, (size_t)ni * 8, cudaMemcpyHostToDevice, sl->st) != cudaSuccess)
+        return SG_ERR_CUDA;
+    for (d = 1; d <= SG_MAX_DIMS; d++) {
+        if (!count[d]) continue;
+        e = sgk_evaluate_batch(d, sl->d_args, sl->d_items + 2 * (int64_t)first[d], count[d], 2, sl->st);
+        if (e != cudaSuccess) return SG_ERR_CUDA;
+    }
+    if (cudaMemcpyAsync(sl->h_out, sl->d_out, (size_t)pts * 4, cudaMemcpyDeviceToHost, sl->st) != cudaSuccess ||
+        cudaEventRecord(sl->done, sl->st) != cudaSuccess)
+        return SG_ERR_CUDA;
+    return SG_OK;
+}
+
+static void *dispatcher(void *arg)
+{
+    sg_server *s = (sg_server *)arg;
+    cudaSetDevice(s->dev);
+    pthread_mutex_lock(&s->mu);
+    while (s->running) {
+        int i, any_busy = 0, free_slot = -1;
+        for (i = 0; i < SRV_SLOTS; i++) {
+            srv_slot *sl = &s->slot[(s->st_batches + i) % SRV_SLOTS];
+            if (sl->busy) {
+                cudaError_t q = cudaEventQuery(sl->done);
+                if (q == cudaSuccess) finish_slot(s, sl, 1);
+                else if (q != cudaErrorNotReady) {
+                    finish_slot(s, sl, 0);
+                    s->fatal = 1;
+                }
+            }
+        }
+        for (i = 0; i < SRV_SLOTS; i++) {
+            if (s->slot[i].busy) any_busy = 1;
+            else if (free_slot < 0) free_slot = i;
+        }
+        if (s->head && free_slot >= 0 && !s->fatal) {
+            srv_slot *sl = &s->slot[free_slot];
+            take_batch(s, sl);
+            sl->busy = 1;
+            s->st_batches++;
+            s->st_requests += sl->nreq;
+            pthread_mutex_unlock(&s->mu);
+            i = launch_batch(s, sl);
+            pthread_mutex_lock(&s->mu);
+            if (i != SG_OK) {
+                finish_slot(s, sl, 0);
+                s->fatal = 1;
+            }
+            continue;
+        }
+        if (any_busy) {
+            /* poll the running batches, wake early on new work */
+            struct timespec ts;
+            clock_gettime(CLOCK_REALTIME, &ts);
+            ts.tv_nsec += 20000;
+            if (ts.tv_nsec >= 1000000000L) {
+                ts.tv_sec++;
+                ts.tv_nsec -= 1000000000L;
+            }
+            pthread_cond_timedwait(&s->cv_work, &s->mu, &ts);
+        } else {
+            pthread_cond_wait(&s->cv_work, &s->mu);
+        }
+    }
+    /* drain: wait for running batches, fail what is still queued */
+    for (int i = 0; i < SRV_SLOTS; i++)
+        if (s->slot[i].busy) {
+            pthread_mutex_unlock(&s->mu);
+            cudaEventSynchronize(s->slot[i].done);
+            pthread_mutex_lock(&s->mu);
+            finish_slot(s, &s->slot[i], 1);
+        }
+    while (s->head) {
+        srv_req *r = s->head;
+        s->head = r->next;
+        r->state = 3;
+        s->grids[r->gi].pins--;
+    }
+    s->tail = NULL;
+    pthread_cond_broadcast(&s->cv_done);
+    pthread_mutex_unlock(&s->mu);
+    return NULL;
+}
+
+static void free_slots(sg_server *s)
+{
+    int i;
+    for (i = 0; i < SRV_SLOTS; i++) {
+        srv_slot *sl = &s->slot[i];
+        if (sl->st) cudaStreamDestroy(sl->st);
+        if (sl->done) cudaEventDestroy(sl->done);
+        cudaFreeHost(sl->h_coords);
+        cudaFreeHost(sl->h_out);
+        cudaFreeHost(sl->h_args);
+        cudaFreeHost(sl->h_items);
+        cudaFree(sl->d_coords);
+        cudaFree(sl->d_out);
+        cudaFree(sl->d_args);
+        cudaFree(sl->d_items);
+    }
+}
+
+SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_server **out)
+{
+    sg_server *s;
+    int i;
+    int64_t max_items;
+    if (!out || hbm_cap_bytes <= 0 || max_batch_points < 1 || max_batch_points > ((int64_t)1 << 28))
+        return sfail(SG_ERR_ARG, "sg_server_create: bad argument");
+    *out = NULL;
+    s = (sg_server *)calloc(1, sizeof(sg_server));
+    if (!s) return sfail(SG_ERR_NOMEM, "sg_server_create: out of host memory");
+    if (cudaGetDevice(&s->dev) != cudaSuccess) {
+        free(s);
+        return sfail(SG_ERR_CUDA, "sg_server_create: no CUDA device");
+    }
+    s->cap_bytes = hbm_cap_bytes;
+    s->max_points = max_batch_points;
+    max_items = (max_batch_points + SG_SERVER_CTA_POINTS - 1) / SG_SERVER_CTA_POINTS + SRV_MAX_REQS;
+    pthread_mutex_init(&s->mu, NULL);
+    pthread_mutex_init(&s->plain_mu, NULL);
+    pthread_cond_init(&s->cv_work, NULL);
+    pthread_cond_init(&s->cv_done, NULL);
+    for (i = 0; i < SRV_SLOTS; i++) {
+        srv_slot *sl = &s->slot[i];
+        const size_t cb = (size_t)max_batch_points * SG_MAX_DIMS * 4, ob = (size_t)max_batch_points * 4;
+        if (cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_coords, cb) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_out, ob) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_args, SRV_MAX_REQS * sizeof(sg_eval_args)) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_items, (size_t)max_items * 8) != cudaSuccess ||
+            cudaMalloc((void **)&sl->d_coords, cb) != cudaSuccess || cudaMalloc((void **)&sl->d_out, ob) != cudaSuccess ||
+            cudaMalloc((void **)&sl->d_args, SRV_MAX_REQS * sizeof(sg_eval_args)) != cudaSuccess ||
+            cudaMalloc((void **)&sl->d_items, (size_t)max_items * 8) != cudaSuccess) {
+            cudaGetLastError();
+            free_slots(s);
+            free(s);
+            return sfail(SG_ERR_NOMEM, "sg_server_create: cannot allocate batch buffers for %lld points",
+                         (long long)max_batch_points);
+        }
+    }
+    if (cudaStreamCreateWithFlags(&s->admit_st, cudaStreamNonBlocking) != cudaSuccess) {
+        free_slots(s);
+        free(s);
+        return sfail(SG_ERR_CUDA, "sg_server_create: stream");
+    }
+    s->running = 1;
+    if (pthread_create(&s->thr, NULL, dispatcher, s) != 0) {
+        cudaStreamDestroy(s->admit_st);
+        free_slots(s);
+        free(s);
+        return sfail(SG_ERR_STATE, "sg_server_create: cannot start the dispatcher thread");
+    }
+    s->thread_ok = 1;
+    *out = s;
+    return SG_OK;
+}
+
+SG_API int sg_server_destroy(sg_server *s)
+{
+    int i;
+    int64_t t;
+    if (!s) return SG_OK;
+    pthread_mutex_lock(&s->mu);
+    s->running = 0;
+    pthread_cond_broadcast(&s->cv_work);
+    pthread_mutex_unlock(&s->mu);
+    if (s->thread_ok) pthread_join(s->thr, NULL);
+    for (i = 0; i < s->ngrids; i++)
+        if (s->grids[i].alive) sg_destroy(s->grids[i].g);
+    for (t = 0; t < s->next_ticket; t++) free(s->by_ticket[t]);
+    free(s->by_ticket);
+    free(s->grids);
+    cudaStreamDestroy(s->admit_st);
+    free_slots(s);
+    pthread_cond_destroy(&s->cv_work);
+    pthread_cond_destroy(&s->cv_done);
+    pthread_mutex_destroy(&s->mu);
+    pthread_mutex_destroy(&s->plain_mu);
+    free(s);
+    return SG_OK;
+}
+
+/* device bytes a grid will take once resident (values, block layout and
+ * tables), from its host layout */
+static int64_t grid_bytes_estimate(const sg_layout *L)
+{
+    return L->Npad * 4 + L->N * 4 + L->S * (int64_t)(sizeof(sg_repack) + 12 * L->d) + (1 << 16);
+}
+
+/* Frees LRU grids nobody needs until `need` more bytes fit (lock held). */
+static int make_room(sg_server *s, int64_t need)
+{
+    while (s->used_bytes + need > s->cap_bytes) {
+        int i, victim = -1;
+        for (i = 0; i < s->ngrids; i++) {
+            const srv_grid *e = &s->grids[i];
+            if (e->alive && e->pins == 0 && (victim < 0 || e->last_used < s->grids[victim].last_used)) victim = i;
+        }
+        if (victim < 0) return 0;
+        sg_destroy(s->grids[victim].g);
+        s->grids[victim].g = NULL;
+        s->grids[victim].alive = 0;
+        s->used_bytes -= s->grids[victim].bytes;
+        s->st_evictions++;
+    }
+    return 1;
+}
+
+SG_API int sg_server_add_grid(sg_server *s, int d, int n, const int *limits, int fn, const double *params,
+                              int num_params, int64_t *grid_id)
+{
+    sg_grid *g = NULL;
+    sg_layout L;
+    int64_t est, bytes = 0;
+    int r, slot;
+    if (!s || !grid_id) return sfail(SG_ERR_ARG, "sg_server_add_grid: NULL argument");
+    if ((r = sg_layout_init(&L, d, n, limits)) != SG_OK) return sfail(r, "sg_server_add_grid: bad grid shape");
+    est = grid_bytes_estimate(&L);
+    pthread_mutex_lock(&s->mu);
+    if (!make_room(s, est)) {
+        pthread_mutex_unlock(&s->mu);
+        return sfail(SG_ERR_NOMEM, "sg_server_add_grid: %lld bytes do not fit under the cap (%lld used of %lld)",
+                     (long long)est, (long long)s->used_bytes, (long long)s->cap_bytes);
+    }
+    s->used_bytes += est; /* reserved while the grid is built */
+    pthread_mutex_unlock(&s->mu);
+
+    r = sg_create(d, n, limits, &g);
+    if (r == SG_OK) r = sg_sample_function(g, fn, params, num_params, s->admit_st);
+    if (r == SG_OK) r = sg_hierarchize_async(g, s->admit_st);
+    if (r == SG_OK) r = sg_grid_prepare_eval(g, s->admit_st);
+    if (r == SG_OK) r = sg_sync(g, s->admit_st);
+    if (r == SG_OK) r = sg_device_bytes(g, &bytes);
+
+    pthread_mutex_lock(&s->mu);
+    s->used_bytes -= est;
+    if (r != SG_OK) {
+        pthread_mutex_unlock(&s->mu);
+        sg_destroy(g);
+        return r;
+    }
+    if (s->ngrids == s->cap_grids) {
+        int nc = s->cap_grids ? 2 * s->cap_grids : 64;
+        srv_grid *ng = (srv_grid *)realloc(s->grids, (size_t)nc * sizeof(srv_grid));
+        if (!ng) {
+            pthread_mutex_unlock(&s->mu);
+            sg_destroy(g);
+            return sfail(SG_ERR_NOMEM, "sg_server_add_grid: out of host memory");
+        }
+        s->grids = ng;
+        s->cap_grids = nc;
+    }
+    slot = s->ngrids++;
+    s->grids[slot].id = s->next_id++;
+    s->grids[slot].g = g;
+    s->grids[slot].bytes = bytes;
+    s->grids[slot].last_used = ++s->clock;
+    s->grids[slot].pins = 0;
+    s->grids[slot].alive = 1;
+    s->used_bytes += bytes;
+    *grid_id = s->grids[slot].id;
+    pthread_mutex_unlock(&s->mu);
+    return SG_OK;
+}
+
+static int find_grid(const sg_server *s, int64_t id)
+{
+    /* ids are handed out in table order */
+    if (id < 0 || id >= s->ngrids || s->grids[id].id != id) return -1;
+    return (int)id;
+}
+
+SG_API int sg_server_submit(sg_server *s, int64_t grid_id, const float *coord_mat, int64_t num_evals, float *out,
+                            int64_t *ticket)
+{
+    srv_req *r;
+    int gi;
+    if (!s || !ticket || num_evals < 1 || !coord_mat || !out) return sfail(SG_ERR_ARG, "sg_server_submit: bad argument");
+    if (num_evals > s->max_points)
+        return sfail(SG_ERR_RANGE, "sg_server_submit: %lld points exceed the batch capacity %lld", (long long)num_evals,
+                     (long long)s->max_points);
+    r = (srv_req *)calloc(1, sizeof(srv_req));
+    if (!r) return sfail(SG_ERR_NOMEM, "sg_server_submit: out of host memory");
+    pthread_mutex_lock(&s->mu);
+    gi = find_grid(s, grid_id);
+    if (gi < 0 || !s->grids[gi].alive || s->fatal) {
+        pthread_mutex_unlock(&s->mu);
+        free(r);
+        return sfail(s->fatal ? SG_ERR_CUDA : SG_ERR_ARG, "sg_server_submit: grid %lld is not resident",
+                     (long long)grid_id);
+    }
+    if (s->next_ticket == s->cap_tickets) {
+        int64_t nc = s->cap_tickets ? 2 * s->cap_tickets : 4096;
+        srv_req **nb = (srv_req **)realloc(s->by_ticket, (size_t)nc * sizeof(srv_req *));
+        if (!nb) {
+            pthread_mutex_unlock(&s->mu);
+            free(r);
+            return sfail(SG_ERR_NOMEM, "sg_server_submit: out of host memory");
+        }
+        s->by_ticket = nb;
+        s->cap_tickets = nc;
+    }
+    r->ticket = s->next_ticket++;
+    s->by_ticket[r->ticket] = r;
+    r->gi = gi;
+    r->d = s->grids[gi].g->L.d;
+    r->coords = coord_mat;
+    r->out = out;
+    r->m = num_evals;
+    r->t_submit = now_ms();
+    s->grids[gi].pins++;
+    s->grids[gi].last_used = ++s->clock;
+    if (s->tail) s->tail->next = r;
+    else s->head = r;
+    s->tail = r;
+    s->queued_points += num_evals;
+    s->st_points += num_evals;
+    *ticket = r->ticket;
+    pthread_cond_signal(&s->cv_work);
+    pthread_mutex_unlock(&s->mu);
+    return SG_OK;
+}
+
+SG_API int sg_server_wait(sg_server *s, int64_t ticket, double *latency_ms)
+{
+    srv_req *r;
+    int st;
+    if (!s) return sfail(SG_ERR_ARG, "sg_server_wait: NULL server");
+    pthread_mutex_lock(&s->mu);
+    if (ticket < 0 || ticket >= s->next_ticket || !(r = s->by_ticket[ticket])) {
+        pthread_mutex_unlock(&s->mu);
+        return sfail(SG_ERR_ARG, "sg_server_wait: unknown or already collected ticket %lld", (long long)ticket);
+    }
+    while (r->state < 2) pthread_cond_wait(&s->cv_done, &s->mu);
+    st = r->state;
+    if (latency_ms) *latency_ms = r->t_done - r->t_submit;
+    s->by_ticket[ticket] = NULL;
+    pthread_mutex_unlock(&s->mu);
+    free(r);
+    return st == 2 ? SG_OK : sfail(SG_ERR_CUDA, "sg_server_wait: the request failed");
+}
+
+SG_API int sg_server_stats(sg_server *s, int64_t *stats)
+{
+    int i;
+    int64_t resident = 0;
+    if (!s || !stats) return sfail(SG_ERR_ARG, "sg_server_stats: NULL argument");
+    pthread_mutex_lock(&s->mu);
+    for (i = 0; i < s->ngrids; i++) resident += s->grids[i].alive;
+    stats[0] = s->st_batches;
+    stats[1] = s->st_requests;
+    stats[2] = s->st_points;
+    stats[3] = s->st_evictions;
+    stats[4] = resident;
+    stats[5] = s->used_bytes;
+    stats[6] = s->st_failed;
+    pthread_mutex_unlock(&s->mu);
+    return SG_OK;
+}
+
+SG_API int sg_server_evaluate_now(sg_server *s, int64_t grid_id, const float *coord_mat, int64_t num_evals, float *out)
+{
+    /* the plain arrangement, for comparison: this one request alone through
+     * the single-grid host-buffer call */
+    int gi, r;
+    sg_grid *g;
+    if (!s) return sfail(SG_ERR_ARG, "sg_server_evaluate_now: NULL server");
+    pthread_mutex_lock(&s->mu);
+    gi = find_grid(s, grid_id);
+    if (gi < 0 || !s->grids[gi].alive) {
+        pthread_mutex_unlock(&s->mu);
+        return sfail(SG_ERR_ARG, "sg_server_evaluate_now: grid %lld is not resident", (long long)grid_id);
+    }
+    g = s->grids[gi].g;
+    s->grids[gi].pins++;
+    s->grids[gi].last_used = ++s->clock;
+    pthread_mutex_unlock(&s->mu);
+    pthread_mutex_lock(&s->plain_mu);
+    r = sg_evaluate(g, coord_mat, out, num_evals);
+    pthread_mutex_unlock(&s->plain_mu);
+    pthread_mutex_lock(&s->mu);
+    s->grids[gi].pins--;
+    pthread_mutex_unlock(&s->mu);
+    return r;
+}

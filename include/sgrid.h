@@ -195,6 +195,40 @@ int sg_batch_sync(sg_batch *batch, void *stream);
 int sg_batch_set_option(sg_batch *batch, int option, int64_t value);
 int sg_batch_device_bytes(const sg_batch *batch, int64_t *bytes);
 
+/* ---- serving loop --------------------------------------------------------
+ * A pool of hierarchized grids resident on the current device under a byte
+ * cap, and a dispatcher thread that batches evaluate requests continuously:
+ * every request queued when a batch slot frees up goes into one batch (one
+ * copy in, one batched launch per dimension, one copy out); two slots
+ * alternate so one batch is assembled while the other computes.  No
+ * reference counterpart. */
+typedef struct sg_server sg_server;
+/* max_batch_points: points per batch (and the largest single request) */
+int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_server **server);
+/* Stops the dispatcher (running batches finish, queued requests fail) and
+ * frees every resident grid. */
+int sg_server_destroy(sg_server *server);
+/* Admits a grid: create, sample fn (sg_sample_function), hierarchize, build
+ * the evaluation layout.  Evicts least recently used grids with no queued or
+ * running request while the cap would be exceeded; SG_ERR_NOMEM if that is
+ * not enough.  Blocks until the grid is ready. */
+int sg_server_add_grid(sg_server *server, int d, int n, const int *limits, int fn, const double *params,
+                       int num_params, int64_t *grid_id);
+/* Queues out[0..num_evals) = grid at coord_mat (host buffers that must stay
+ * valid until sg_server_wait returns for the ticket).  Never blocks on the
+ * GPU.  SG_ERR_ARG if the grid is not resident. */
+int sg_server_submit(sg_server *server, int64_t grid_id, const float *coord_mat, int64_t num_evals,
+                     float *out, int64_t *ticket);
+/* Waits for a ticket; latency_ms (optional) = submit -> results in `out`. */
+int sg_server_wait(sg_server *server, int64_t ticket, double *latency_ms);
+/* stats[7]: batches, requests, points, evictions, resident grids, bytes in
+ * use, failed requests */
+int sg_server_stats(sg_server *server, int64_t *stats);
+/* The request alone through sg_evaluate on the resident grid (the plain
+ * one-launch-per-request arrangement; for comparison). */
+int sg_server_evaluate_now(sg_server *server, int64_t grid_id, const float *coord_mat, int64_t num_evals,
+                           float *out);
+
 /* ---- options and diagnostics ------------------------------------------ */
 int sg_set_option(sg_grid *grid, int option, int64_t value);
 int sg_get_option(const sg_grid *grid, int option, int64_t *value);

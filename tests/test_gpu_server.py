@@ -1,0 +1,114 @@
+"""The serving loop on the GPU: results equal the single-grid evaluation,
+each request's result is the same alone and in a mix of concurrent requests,
+LRU eviction under the byte cap, submissions from several host threads."""
+import threading
+
+import numpy as np
+import pytest
+
+import adaptive_sparse_grid_bench_b200 as sg
+from adaptive_sparse_grid_bench_b200 import _lib, inputs
+
+pytestmark = pytest.mark.gpu
+
+SHAPES = [(4, 8, _lib.SG_FN_PROD4, ()), (10, 5, _lib.SG_FN_GAUSS, ()), (2, 9, _lib.SG_FN_BUMP, (0.3, 50.0)),
+          (7, 6, _lib.SG_FN_GAUSS, ()), (12, 4, _lib.SG_FN_PROD4, ())]
+
+
+def _server(cap=8 << 30):
+    srv = sg.Server(cap, max_batch_points=1 << 18)
+    ids = [srv.add_grid(d, n, fn, p) for d, n, fn, p in SHAPES]
+    return srv, ids
+
+
+def test_server_results_equal_single_grid(cuda):
+    srv, ids = _server()
+    rng_seed = 40
+    tickets = []
+    for q in range(40):
+        g = q % len(ids)
+        m = [1, 17, 512, 513, 3000, 65536][q % 6]
+        X = inputs.uniform_points(rng_seed + q, m, SHAPES[g][0])
+        tickets.append((g, X, srv.submit(ids[g], X)))
+    for g, X, t in tickets:
+        out, lat = srv.wait(t)
+        want = srv.evaluate_now(ids[g], X)
+        assert lat >= 0
+        assert np.array_equal(out.view(np.uint32), want.view(np.uint32))
+    st = srv.stats()
+    assert st["requests"] == 40 and st["failed"] == 0 and st["batches"] >= 1
+    srv.close()
+
+
+def test_same_result_alone_and_in_mix(cuda):
+    srv, ids = _server()
+    X = inputs.uniform_points(7, 20000, SHAPES[1][0])
+    alone, _ = srv.wait(srv.submit(ids[1], X))
+    mix = []
+    for q in range(64):
+        g = q % len(ids)
+        mix.append(srv.submit(ids[g], inputs.uniform_points(100 + q, 1 + 997 * q % 40000, SHAPES[g][0])))
+        if q == 31:
+            mine = srv.submit(ids[1], X)
+    for t in mix:
+        srv.wait(t)
+    in_mix, _ = srv.wait(mine)
+    assert np.array_equal(alone.view(np.uint32), in_mix.view(np.uint32))
+    assert srv.stats()["batches"] >= 2
+    srv.close()
+
+
+def test_lru_eviction_under_cap(cuda):
+    probe = sg.Grid(6, 10)
+    probe.sample_function(_lib.SG_FN_GAUSS)
+    probe.hierarchize()
+    one = probe.device_bytes()  # about 8 MB
+    srv = sg.Server(int(2.5 * one), max_batch_points=1 << 16)
+    a = srv.add_grid(6, 10, _lib.SG_FN_GAUSS)
+    b = srv.add_grid(6, 10, _lib.SG_FN_PROD4)
+    X = inputs.uniform_points(1, 100, 6)
+    srv.wait(srv.submit(a, X))  # a is now the most recently used
+    c = srv.add_grid(6, 10, _lib.SG_FN_GAUSS)  # evicts b (least recently used)
+    st = srv.stats()
+    assert st["evictions"] == 1 and st["resident_grids"] == 2
+    srv.wait(srv.submit(a, X))
+    srv.wait(srv.submit(c, X))
+    with pytest.raises(sg.SgError):
+        srv.submit(b, X)
+    with pytest.raises(sg.SgError) as e:
+        srv.add_grid(10, 10, _lib.SG_FN_GAUSS)  # larger than the whole cap
+    assert e.value.code == _lib.SG_ERR_NOMEM
+    srv.close()
+
+
+def test_submissions_from_several_threads(cuda):
+    srv, ids = _server()
+    errors = []
+
+    def client(k):
+        try:
+            for q in range(25):
+                g = (k + q) % len(ids)
+                X = inputs.uniform_points(1000 * k + q, 1 + (q * 131) % 5000, SHAPES[g][0])
+                out, _ = srv.wait(srv.submit(ids[g], X))
+                if not np.array_equal(out, srv.evaluate_now(ids[g], X)):
+                    errors.append((k, q))
+        except Exception as exc:  # pragma: no cover - reported below
+            errors.append(repr(exc))
+
+    th = [threading.Thread(target=client, args=(k,)) for k in range(4)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=120)
+    assert not errors
+    srv.close()
+
+
+def test_request_larger_than_batch_is_rejected(cuda):
+    srv = sg.Server(1 << 30, max_batch_points=1024)
+    g = srv.add_grid(3, 4, _lib.SG_FN_PROD4)
+    with pytest.raises(sg.SgError) as e:
+        srv.submit(g, np.zeros((1025, 3), np.float32))
+    assert e.value.code == _lib.SG_ERR_RANGE
+    srv.close()
