@@ -11,6 +11,14 @@
 
 #define NOPT 8
 
+/* Device allocator hooks.  A handle made by sg_create uses cudaMalloc and
+ * cudaFree; the serving loop hands its grids a sub-allocator over one
+ * reserved range instead, so admitting and evicting grids never calls the
+ * CUDA allocator (whose frees wait for the whole device).  alloc returns an
+ * SG_* code and sets *ptr (256-byte aligned); free accepts NULL. */
+typedef int (*sg_dev_alloc_fn)(void *ctx, void **ptr, int64_t bytes);
+typedef void (*sg_dev_free_fn)(void *ctx, void *ptr);
+
 struct sg_grid {
     sg_layout L;
     int dev;        /* device of the device state, -1 before it exists */
@@ -34,7 +42,14 @@ struct sg_grid {
     int64_t dev_bytes;
     cudaEvent_t ev[SG_NUM_PHASES][2]; /* profiling: start/stop per phase */
     int ev_used[SG_NUM_PHASES];
+    sg_dev_alloc_fn alloc; /* NULL: cudaMalloc/cudaFree */
+    sg_dev_free_fn free_fn;
+    void *alloc_ctx;
 };
+
+/* sg_create with the handle's device memory taken from alloc/free_fn. */
+int sg_create_with_allocator(int d, int n, const int *limits, sg_dev_alloc_fn alloc, sg_dev_free_fn free_fn,
+                             void *ctx, sg_grid **grid);
 
 
 /* Builds the block layout if the values changed since it was last built. */

@@ -72,6 +72,13 @@ SG_API int sg_create(int d, int n, const int *limits, sg_grid **grid)
     return SG_OK;
 }
 
+static void dev_free(sg_grid *g, void *p)
+{
+    if (!p) return;
+    if (g->free_fn) g->free_fn(g->alloc_ctx, p);
+    else cudaFree(p);
+}
+
 static void free_device(sg_grid *g)
 {
     int k;
@@ -83,17 +90,30 @@ static void free_device(sg_grid *g)
             cudaEventDestroy(g->ev[k][1]);
             g->ev[k][0] = g->ev[k][1] = NULL;
         }
-    cudaFree(g->d_alpha);
-    cudaFree(g->d_work);
-    cudaFree(g->d_blk);
-    cudaFree(g->d_repack);
+    dev_free(g, g->d_alpha);
+    dev_free(g, g->d_work);
+    dev_free(g, g->d_blk);
+    dev_free(g, g->d_repack);
     for (k = 0; k < SG_MAX_DIMS; k++) {
-        cudaFree(g->d_chains[k]);
-        cudaFree(g->d_seg[k]);
+        dev_free(g, g->d_chains[k]);
+        dev_free(g, g->d_seg[k]);
     }
-    cudaFree(g->d_err);
-    cudaFree(g->d_scratch);
-    cudaFree(g->d_io);
+    dev_free(g, g->d_err);
+    dev_free(g, g->d_scratch);
+    dev_free(g, g->d_io);
+}
+
+int sg_create_with_allocator(int d, int n, const int *limits, sg_dev_alloc_fn alloc, sg_dev_free_fn free_fn,
+                             void *ctx, sg_grid **grid)
+{
+    int r;
+    if (!alloc || !free_fn) return fail(SG_ERR_ARG, "sg_create_with_allocator: allocator hooks are NULL");
+    r = sg_create(d, n, limits, grid);
+    if (r != SG_OK) return r;
+    (*grid)->alloc = alloc;
+    (*grid)->free_fn = free_fn;
+    (*grid)->alloc_ctx = ctx;
+    return SG_OK;
 }
 
 SG_API int sg_destroy(sg_grid *g)
@@ -194,7 +214,17 @@ SG_API int sg_idx2l(const sg_grid *g, int64_t pos, int s, int *lv)
 
 static int dev_alloc(sg_grid *g, void **p, int64_t bytes, const char *what)
 {
-    cudaError_t e = cudaMalloc(p, (size_t)(bytes > 0 ? bytes : 16));
+    cudaError_t e;
+    if (g->alloc) {
+        int r = g->alloc(g->alloc_ctx, p, bytes > 0 ? bytes : 16);
+        if (r != SG_OK) {
+            *p = NULL;
+            return fail(r, "allocating %lld bytes for %s from the handle's allocator", (long long)bytes, what);
+        }
+        g->dev_bytes += bytes;
+        return SG_OK;
+    }
+    e = cudaMalloc(p, (size_t)(bytes > 0 ? bytes : 16));
     if (e != cudaSuccess) {
         *p = NULL;
         cudaGetLastError();
@@ -219,17 +249,29 @@ static void leave(sg_grid *g, int prev)
     if (g->dev >= 0 && g->dev != prev) cudaSetDevice(prev);
 }
 
-static int materialize(sg_grid *g)
+/* Allocates the handle's device state and uploads its tables.  The clears
+ * and uploads go on `st` (the stream of the call that needs the state, never
+ * the legacy default stream, so a serving loop's streams do not wait on
+ * them), and the stream is synchronized before returning, so kernels on any
+ * stream may read the tables afterwards. */
+static int materialize(sg_grid *g, cudaStream_t st)
 {
     const sg_layout *L = &g->L;
     sg_repack *rp = NULL;
     int k, r;
+    cudaError_t ce;
     if (g->dev >= 0) return SG_OK;
     CU(cudaGetDevice(&g->dev), "cudaGetDevice");
     if ((r = dev_alloc(g, (void **)&g->d_alpha, L->Npad * 4, "grid values")) != SG_OK) goto bad;
-    CU(cudaMemset(g->d_alpha, 0, (size_t)L->Npad * 4), "cudaMemset");
+    if ((ce = cudaMemsetAsync(g->d_alpha, 0, (size_t)L->Npad * 4, st)) != cudaSuccess) {
+        r = cuda_fail(ce, "cudaMemsetAsync");
+        goto bad;
+    }
     if ((r = dev_alloc(g, (void **)&g->d_err, 16, "error flag")) != SG_OK) goto bad;
-    CU(cudaMemset(g->d_err, 0, 16), "cudaMemset");
+    if ((ce = cudaMemsetAsync(g->d_err, 0, 16, st)) != cudaSuccess) {
+        r = cuda_fail(ce, "cudaMemsetAsync");
+        goto bad;
+    }
     if ((r = sg_layout_eval_tables(L, &rp, g->blk3, g->blk2)) != SG_OK) {
         fail(r, "building the evaluation layout tables");
         goto bad;
@@ -237,7 +279,12 @@ static int materialize(sg_grid *g)
     if ((r = dev_alloc(g, (void **)&g->d_blk, L->N * 4, "block layout")) != SG_OK) goto bad;
     if ((r = dev_alloc(g, (void **)&g->d_repack, L->S * (int64_t)sizeof(sg_repack), "repack table")) != SG_OK)
         goto bad;
-    CU(cudaMemcpy(g->d_repack, rp, (size_t)L->S * sizeof(sg_repack), cudaMemcpyHostToDevice), "cudaMemcpy");
+    /* pageable sources: the copy has taken the bytes when the call returns */
+    if ((ce = cudaMemcpyAsync(g->d_repack, rp, (size_t)L->S * sizeof(sg_repack), cudaMemcpyHostToDevice, st)) !=
+        cudaSuccess) {
+        r = cuda_fail(ce, "uploading the repack table");
+        goto bad;
+    }
     free(rp);
     rp = NULL;
     g->eval_dirty = 1;
@@ -265,8 +312,9 @@ static int materialize(sg_grid *g)
         r = dev_alloc(g, (void **)&g->d_chains[k], nch * (int64_t)sizeof(sg_chain), "sweep chains");
         if (r == SG_OK) r = dev_alloc(g, (void **)&g->d_seg[k], nseg * 4, "sweep segments");
         if (r == SG_OK && nch > 0) {
-            cudaError_t e = cudaMemcpy(g->d_chains[k], ch, (size_t)nch * sizeof(sg_chain), cudaMemcpyHostToDevice);
-            if (e == cudaSuccess) e = cudaMemcpy(g->d_seg[k], seg, (size_t)nseg * 4, cudaMemcpyHostToDevice);
+            cudaError_t e =
+                cudaMemcpyAsync(g->d_chains[k], ch, (size_t)nch * sizeof(sg_chain), cudaMemcpyHostToDevice, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(g->d_seg[k], seg, (size_t)nseg * 4, cudaMemcpyHostToDevice, st);
             if (e != cudaSuccess) r = cuda_fail(e, "uploading sweep tables");
         }
         free(ch);
@@ -279,8 +327,13 @@ static int materialize(sg_grid *g)
         g->sweep[k].cap32 = cap32;
         g->sweep[k].cap64 = cap64;
     }
+    if ((ce = cudaStreamSynchronize(st)) != cudaSuccess) {
+        r = cuda_fail(ce, "uploading the grid tables");
+        goto bad;
+    }
     return SG_OK;
 bad:
+    cudaStreamSynchronize(st); /* nothing may still write the ranges freed below */
     free(rp);
     free_device(g);
     memset(g->d_chains, 0, sizeof(g->d_chains));
@@ -320,7 +373,7 @@ SG_API int sg_set_values(sg_grid *g, const float *values)
     int prev, r;
     if (!g || !values) return fail(SG_ERR_ARG, "sg_set_values: NULL argument");
     if ((r = enter(g, &prev)) != SG_OK) return r;
-    if ((r = materialize(g)) == SG_OK &&
+    if ((r = materialize(g, 0)) == SG_OK &&
         (r = copy_groups(g, g->d_alpha, values, 1, cudaMemcpyHostToDevice, 0)) == SG_OK) {
         cudaError_t e = cudaStreamSynchronize(0);
         if (e != cudaSuccess) r = cuda_fail(e, "sg_set_values");
@@ -335,7 +388,7 @@ SG_API int sg_set_values_device(sg_grid *g, const float *values, void *stream)
     int prev, r;
     if (!g || !values) return fail(SG_ERR_ARG, "sg_set_values_device: NULL argument");
     if ((r = enter(g, &prev)) != SG_OK) return r;
-    if ((r = materialize(g)) == SG_OK &&
+    if ((r = materialize(g, (cudaStream_t)stream)) == SG_OK &&
         (r = copy_groups(g, g->d_alpha, values, 1, cudaMemcpyDeviceToDevice, (cudaStream_t)stream)) == SG_OK)
         g->has_values = 1, g->eval_dirty = 1;
     leave(g, prev);
@@ -460,11 +513,12 @@ SG_API int sg_sync(sg_grid *g, void *stream)
     if (!g) return fail(SG_ERR_ARG, "sg_sync: NULL grid");
     if (g->dev < 0) return SG_OK;
     if ((r = enter(g, &prev)) != SG_OK) return r;
-    e = cudaStreamSynchronize((cudaStream_t)stream);
-    if (e == cudaSuccess) e = cudaMemcpy(&flag, g->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    e = cudaMemcpyAsync(&flag, g->d_err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize((cudaStream_t)stream);
     if (e != cudaSuccess) r = cuda_fail(e, "sg_sync");
     else if (flag) {
-        cudaMemset(g->d_err, 0, sizeof(int));
+        cudaMemsetAsync(g->d_err, 0, sizeof(int), (cudaStream_t)stream);
+        cudaStreamSynchronize((cudaStream_t)stream);
         r = fail(SG_ERR_TIMEOUT, "a device-side wait gave up; the grid values are not valid");
     }
     leave(g, prev);
@@ -476,7 +530,7 @@ static int ensure(sg_grid *g, void **buf, int64_t *have, int64_t need, const cha
     int r;
     if (*have >= need) return SG_OK;
     if (*buf) {
-        cudaFree(*buf);
+        dev_free(g, *buf);
         g->dev_bytes -= *have;
         *buf = NULL;
         *have = 0;
@@ -646,7 +700,7 @@ SG_API int sg_sample_function(sg_grid *g, int fn, const double *params, int np, 
     }
     if (np < need) return fail(SG_ERR_ARG, "sg_sample_function: function %d needs %d parameters", fn, need);
     if ((r = enter(g, &prev)) != SG_OK) return r;
-    if ((r = materialize(g)) == SG_OK) {
+    if ((r = materialize(g, (cudaStream_t)stream)) == SG_OK) {
         if ((e = sgk_sample(&g->L, fn, params, np, g->d_alpha, stream)) != cudaSuccess)
             r = cuda_fail((cudaError_t)e, "sg_sample_function");
         else

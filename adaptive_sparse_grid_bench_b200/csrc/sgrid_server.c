@@ -3,10 +3,15 @@
  * dispatcher thread.
  *
  * Resident grids: a pool of hierarchized grids kept on the device under a
- * byte cap.  sg_server_add_grid admits a new grid (create, sample,
- * hierarchize, build the evaluation layout) after evicting least recently
- * used grids that no queued or running request needs; if that cannot free
- * enough memory the admission fails with SG_ERR_NOMEM.
+ * byte cap.  The server reserves the whole cap as one device range at
+ * creation and sub-allocates every grid buffer from it (first fit over an
+ * offset-sorted free list, neighbours merged on free), so admitting and
+ * evicting grids makes no cudaMalloc/cudaFree call: a cudaFree waits for the
+ * whole device, which would stall the batches in flight.
+ * sg_server_add_grid admits a new grid (create, sample, hierarchize, build
+ * the evaluation layout) after evicting least recently used grids that no
+ * queued or running request needs; if that cannot free enough memory the
+ * admission fails with SG_ERR_NOMEM.
  *
  * Continuous batching: callers submit evaluate requests of any size (up to
  * the batch capacity) against resident grids and get a ticket.  The
@@ -35,6 +40,118 @@
 #define SRV_SLOTS 2
 #define SRV_MAX_REQS 8192 /* requests per batch */
 #define SG_SERVER_CTA_POINTS 512 /* points per CTA of the batched kernel at 2 per thread */
+
+#define ARENA_ALIGN 256
+
+typedef struct arena_rng {
+    int64_t off, size;
+} arena_rng;
+
+typedef struct sg_arena {
+    char *base;
+    int64_t size, used;
+    pthread_mutex_t mu;
+    arena_rng *fr; /* free ranges, sorted by offset, never adjacent */
+    int64_t nfr, capfr;
+    arena_rng *live; /* handed-out ranges, unordered */
+    int64_t nlive, caplive;
+} sg_arena;
+
+static int rng_reserve(arena_rng **a, int64_t *cap, int64_t need)
+{
+    arena_rng *na;
+    int64_t nc;
+    if (need <= *cap) return 1;
+    nc = *cap ? 2 * *cap : 256;
+    while (nc < need) nc *= 2;
+    na = (arena_rng *)realloc(*a, (size_t)nc * sizeof(arena_rng));
+    if (!na) return 0;
+    *a = na;
+    *cap = nc;
+    return 1;
+}
+
+static int arena_alloc(void *ctx, void **ptr, int64_t bytes)
+{
+    sg_arena *A = (sg_arena *)ctx;
+    int64_t i, sz = (bytes + ARENA_ALIGN - 1) & ~(int64_t)(ARENA_ALIGN - 1);
+    int r = SG_ERR_NOMEM;
+    *ptr = NULL;
+    pthread_mutex_lock(&A->mu);
+    for (i = 0; i < A->nfr; i++) {
+        arena_rng *f = &A->fr[i];
+        if (f->size < sz) continue;
+        if (!rng_reserve(&A->live, &A->caplive, A->nlive + 1)) break;
+        A->live[A->nlive].off = f->off;
+        A->live[A->nlive].size = sz;
+        A->nlive++;
+        *ptr = A->base + f->off;
+        f->off += sz;
+        f->size -= sz;
+        if (f->size == 0) {
+            memmove(&A->fr[i], &A->fr[i + 1], (size_t)(A->nfr - i - 1) * sizeof(arena_rng));
+            A->nfr--;
+        }
+        A->used += sz;
+        r = SG_OK;
+        break;
+    }
+    pthread_mutex_unlock(&A->mu);
+    return r;
+}
+
+static void arena_free(void *ctx, void *ptr)
+{
+    sg_arena *A = (sg_arena *)ctx;
+    int64_t i, off, sz, lo, hi;
+    if (!ptr) return;
+    off = (char *)ptr - A->base;
+    pthread_mutex_lock(&A->mu);
+    for (i = 0; i < A->nlive && A->live[i].off != off; i++) {
+    }
+    if (i == A->nlive || !rng_reserve(&A->fr, &A->capfr, A->nfr + 1)) {
+        /* not ours (or no host memory to track it): leave it allocated */
+        pthread_mutex_unlock(&A->mu);
+        return;
+    }
+    sz = A->live[i].size;
+    A->live[i] = A->live[--A->nlive];
+    A->used -= sz;
+    /* first free range after off */
+    lo = 0;
+    hi = A->nfr;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) / 2;
+        if (A->fr[mid].off < off) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo > 0 && A->fr[lo - 1].off + A->fr[lo - 1].size == off) {
+        A->fr[lo - 1].size += sz;
+        if (lo < A->nfr && off + sz == A->fr[lo].off) {
+            A->fr[lo - 1].size += A->fr[lo].size;
+            memmove(&A->fr[lo], &A->fr[lo + 1], (size_t)(A->nfr - lo - 1) * sizeof(arena_rng));
+            A->nfr--;
+        }
+    } else if (lo < A->nfr && off + sz == A->fr[lo].off) {
+        A->fr[lo].off = off;
+        A->fr[lo].size += sz;
+    } else {
+        memmove(&A->fr[lo + 1], &A->fr[lo], (size_t)(A->nfr - lo) * sizeof(arena_rng));
+        A->fr[lo].off = off;
+        A->fr[lo].size = sz;
+        A->nfr++;
+    }
+    pthread_mutex_unlock(&A->mu);
+}
+
+static int64_t arena_used(sg_arena *A)
+{
+    int64_t u;
+    pthread_mutex_lock(&A->mu);
+    u = A->used;
+    pthread_mutex_unlock(&A->mu);
+    return u;
+}
 
 typedef struct srv_grid {
     int64_t id;
@@ -78,7 +195,8 @@ struct sg_server {
     int running, thread_ok;
     srv_grid *grids;
     int ngrids, cap_grids;
-    int64_t next_id, cap_bytes, used_bytes;
+    int64_t next_id, cap_bytes;
+    sg_arena arena; /* the cap, reserved once; every grid buffer lives here */
     uint64_t clock;
     srv_req *head, *tail;
     int64_t queued_points;
@@ -278,7 +396,7 @@ static void free_slots(sg_server *s)
 SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_server **out)
 {
     sg_server *s;
-    int i;
+    int i, prio_low = 0, prio_high = 0;
     int64_t max_items;
     if (!out || hbm_cap_bytes <= 0 || max_batch_points < 1 || max_batch_points > ((int64_t)1 << 28))
         return sfail(SG_ERR_ARG, "sg_server_create: bad argument");
@@ -296,10 +414,14 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
     pthread_mutex_init(&s->plain_mu, NULL);
     pthread_cond_init(&s->cv_work, NULL);
     pthread_cond_init(&s->cv_done, NULL);
+    /* batches run at the highest stream priority and admissions at the
+     * lowest, so a long hierarchization of a new grid yields SMs to the
+     * evaluation batches as its CTAs retire */
+    if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess) prio_low = prio_high = 0;
     for (i = 0; i < SRV_SLOTS; i++) {
         srv_slot *sl = &s->slot[i];
         const size_t cb = (size_t)max_batch_points * SG_MAX_DIMS * 4, ob = (size_t)max_batch_points * 4;
-        if (cudaStreamCreateWithFlags(&sl->st, cudaStreamNonBlocking) != cudaSuccess ||
+        if (cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_coords, cb) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_out, ob) != cudaSuccess ||
@@ -315,15 +437,32 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
                          (long long)max_batch_points);
         }
     }
-    if (cudaStreamCreateWithFlags(&s->admit_st, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithPriority(&s->admit_st, cudaStreamNonBlocking, prio_low) != cudaSuccess) {
         free_slots(s);
         free(s);
         return sfail(SG_ERR_CUDA, "sg_server_create: stream");
     }
+    pthread_mutex_init(&s->arena.mu, NULL);
+    s->arena.size = hbm_cap_bytes & ~(int64_t)(ARENA_ALIGN - 1);
+    if (s->arena.size < ARENA_ALIGN || cudaMalloc((void **)&s->arena.base, (size_t)s->arena.size) != cudaSuccess ||
+        !rng_reserve(&s->arena.fr, &s->arena.capfr, 1)) {
+        cudaGetLastError();
+        cudaStreamDestroy(s->admit_st);
+        free_slots(s);
+        free(s->arena.fr);
+        free(s);
+        return sfail(SG_ERR_NOMEM, "sg_server_create: cannot reserve %lld device bytes for resident grids",
+                     (long long)hbm_cap_bytes);
+    }
+    s->arena.fr[0].off = 0;
+    s->arena.fr[0].size = s->arena.size;
+    s->arena.nfr = 1;
     s->running = 1;
     if (pthread_create(&s->thr, NULL, dispatcher, s) != 0) {
         cudaStreamDestroy(s->admit_st);
         free_slots(s);
+        cudaFree(s->arena.base);
+        free(s->arena.fr);
         free(s);
         return sfail(SG_ERR_STATE, "sg_server_create: cannot start the dispatcher thread");
     }
@@ -349,6 +488,10 @@ SG_API int sg_server_destroy(sg_server *s)
     free(s->grids);
     cudaStreamDestroy(s->admit_st);
     free_slots(s);
+    cudaFree(s->arena.base);
+    free(s->arena.fr);
+    free(s->arena.live);
+    pthread_mutex_destroy(&s->arena.mu);
     pthread_cond_destroy(&s->cv_work);
     pthread_cond_destroy(&s->cv_done);
     pthread_mutex_destroy(&s->mu);
@@ -364,23 +507,43 @@ static int64_t grid_bytes_estimate(const sg_layout *L)
     return L->Npad * 4 + L->N * 4 + L->S * (int64_t)(sizeof(sg_repack) + 12 * L->d) + (1 << 16);
 }
 
-/* Frees LRU grids nobody needs until `need` more bytes fit (lock held). */
-static int make_room(sg_server *s, int64_t need)
+/* Evicts the least recently used grid that no request needs (lock held);
+ * returns 0 if every resident grid is pinned. */
+static int evict_one(sg_server *s)
 {
-    while (s->used_bytes + need > s->cap_bytes) {
-        int i, victim = -1;
-        for (i = 0; i < s->ngrids; i++) {
-            const srv_grid *e = &s->grids[i];
-            if (e->alive && e->pins == 0 && (victim < 0 || e->last_used < s->grids[victim].last_used)) victim = i;
-        }
-        if (victim < 0) return 0;
-        sg_destroy(s->grids[victim].g);
-        s->grids[victim].g = NULL;
-        s->grids[victim].alive = 0;
-        s->used_bytes -= s->grids[victim].bytes;
-        s->st_evictions++;
+    int i, victim = -1;
+    for (i = 0; i < s->ngrids; i++) {
+        const srv_grid *e = &s->grids[i];
+        if (e->alive && e->pins == 0 && (victim < 0 || e->last_used < s->grids[victim].last_used)) victim = i;
     }
+    if (victim < 0) return 0;
+    sg_destroy(s->grids[victim].g); /* returns its ranges to the arena: no driver call */
+    s->grids[victim].g = NULL;
+    s->grids[victim].alive = 0;
+    s->st_evictions++;
     return 1;
+}
+
+/* Creates, samples and hierarchizes a grid in the arena and builds its
+ * evaluation layout, all on the admission stream. */
+static int build_grid(sg_server *s, int d, int n, const int *limits, int fn, const double *params, int num_params,
+                      sg_grid **out)
+{
+    sg_grid *g = NULL;
+    int r = sg_create_with_allocator(d, n, limits, arena_alloc, arena_free, &s->arena, &g);
+    if (r == SG_OK) r = sg_sample_function(g, fn, params, num_params, s->admit_st);
+    if (r == SG_OK) r = sg_hierarchize_async(g, s->admit_st);
+    if (r == SG_OK) r = sg_grid_prepare_eval(g, s->admit_st);
+    if (r == SG_OK) r = sg_sync(g, s->admit_st);
+    if (r != SG_OK) {
+        if (g) {
+            cudaStreamSynchronize(s->admit_st); /* nothing of g may still run when its ranges are reused */
+            sg_destroy(g);
+        }
+        return r;
+    }
+    *out = g;
+    return SG_OK;
 }
 
 SG_API int sg_server_add_grid(sg_server *s, int d, int n, const int *limits, int fn, const double *params,
@@ -393,29 +556,30 @@ SG_API int sg_server_add_grid(sg_server *s, int d, int n, const int *limits, int
     if (!s || !grid_id) return sfail(SG_ERR_ARG, "sg_server_add_grid: NULL argument");
     if ((r = sg_layout_init(&L, d, n, limits)) != SG_OK) return sfail(r, "sg_server_add_grid: bad grid shape");
     est = grid_bytes_estimate(&L);
+    if (est > s->arena.size)
+        return sfail(SG_ERR_NOMEM, "sg_server_add_grid: %lld bytes exceed the cap %lld", (long long)est,
+                     (long long)s->arena.size);
     pthread_mutex_lock(&s->mu);
-    if (!make_room(s, est)) {
-        pthread_mutex_unlock(&s->mu);
-        return sfail(SG_ERR_NOMEM, "sg_server_add_grid: %lld bytes do not fit under the cap (%lld used of %lld)",
-                     (long long)est, (long long)s->used_bytes, (long long)s->cap_bytes);
-    }
-    s->used_bytes += est; /* reserved while the grid is built */
+    while (arena_used(&s->arena) + est > s->arena.size)
+        if (!evict_one(s)) break;
     pthread_mutex_unlock(&s->mu);
-
-    r = sg_create(d, n, limits, &g);
-    if (r == SG_OK) r = sg_sample_function(g, fn, params, num_params, s->admit_st);
-    if (r == SG_OK) r = sg_hierarchize_async(g, s->admit_st);
-    if (r == SG_OK) r = sg_grid_prepare_eval(g, s->admit_st);
-    if (r == SG_OK) r = sg_sync(g, s->admit_st);
-    if (r == SG_OK) r = sg_device_bytes(g, &bytes);
+    for (;;) {
+        int evicted;
+        r = build_grid(s, d, n, limits, fn, params, num_params, &g);
+        if (r != SG_ERR_NOMEM) break;
+        /* the free ranges were too fragmented (or another admission took
+         * them): evict one more grid and try again */
+        pthread_mutex_lock(&s->mu);
+        evicted = evict_one(s);
+        pthread_mutex_unlock(&s->mu);
+        if (!evicted)
+            return sfail(SG_ERR_NOMEM, "sg_server_add_grid: %lld bytes do not fit under the cap (%lld used of %lld)",
+                         (long long)est, (long long)arena_used(&s->arena), (long long)s->arena.size);
+    }
+    if (r != SG_OK) return r;
+    sg_device_bytes(g, &bytes);
 
     pthread_mutex_lock(&s->mu);
-    s->used_bytes -= est;
-    if (r != SG_OK) {
-        pthread_mutex_unlock(&s->mu);
-        sg_destroy(g);
-        return r;
-    }
     if (s->ngrids == s->cap_grids) {
         int nc = s->cap_grids ? 2 * s->cap_grids : 64;
         srv_grid *ng = (srv_grid *)realloc(s->grids, (size_t)nc * sizeof(srv_grid));
@@ -434,7 +598,6 @@ SG_API int sg_server_add_grid(sg_server *s, int d, int n, const int *limits, int
     s->grids[slot].last_used = ++s->clock;
     s->grids[slot].pins = 0;
     s->grids[slot].alive = 1;
-    s->used_bytes += bytes;
     *grid_id = s->grids[slot].id;
     pthread_mutex_unlock(&s->mu);
     return SG_OK;
@@ -529,7 +692,7 @@ SG_API int sg_server_stats(sg_server *s, int64_t *stats)
     stats[2] = s->st_points;
     stats[3] = s->st_evictions;
     stats[4] = resident;
-    stats[5] = s->used_bytes;
+    stats[5] = arena_used(&s->arena);
     stats[6] = s->st_failed;
     pthread_mutex_unlock(&s->mu);
     return SG_OK;

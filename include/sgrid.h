@@ -203,7 +203,10 @@ int sg_batch_device_bytes(const sg_batch *batch, int64_t *bytes);
  * alternate so one batch is assembled while the other computes.  No
  * reference counterpart. */
 typedef struct sg_server sg_server;
-/* max_batch_points: points per batch (and the largest single request) */
+/* max_batch_points: points per batch (and the largest single request).
+ * Reserves hbm_cap_bytes of device memory at once (SG_ERR_NOMEM if it is not
+ * free); every resident grid is sub-allocated from that range, so admission
+ * and eviction make no CUDA allocator call. */
 int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_server **server);
 /* Stops the dispatcher (running batches finish, queued requests fail) and
  * frees every resident grid. */
@@ -221,8 +224,8 @@ int sg_server_submit(sg_server *server, int64_t grid_id, const float *coord_mat,
                      float *out, int64_t *ticket);
 /* Waits for a ticket; latency_ms (optional) = submit -> results in `out`. */
 int sg_server_wait(sg_server *server, int64_t ticket, double *latency_ms);
-/* stats[7]: batches, requests, points, evictions, resident grids, bytes in
- * use, failed requests */
+/* stats[7]: batches, requests, points, evictions, resident grids, bytes of
+ * the reserved range in use, failed requests */
 int sg_server_stats(sg_server *server, int64_t *stats);
 /* The request alone through sg_evaluate on the resident grid (the plain
  * one-launch-per-request arrangement; for comparison). */

@@ -112,3 +112,34 @@ def test_request_larger_than_batch_is_rejected(cuda):
         srv.submit(g, np.zeros((1025, 3), np.float32))
     assert e.value.code == _lib.SG_ERR_RANGE
     srv.close()
+
+
+def test_reserved_range_reused_across_evictions(cuda):
+    # a tight cap and grids of mixed size: ranges freed by evictions are
+    # merged and handed to later grids; every admitted grid still evaluates
+    # exactly like a standalone grid of the same shape and function
+    shapes = [(6, 9, _lib.SG_FN_GAUSS, ()), (3, 7, _lib.SG_FN_PROD4, ()), (8, 7, _lib.SG_FN_BUMP, (0.3, 50.0)),
+              (2, 12, _lib.SG_FN_GAUSS, ()), (5, 8, _lib.SG_FN_PROD4, ())]
+    probe = sg.Grid(6, 9)
+    probe.sample_function(_lib.SG_FN_GAUSS)
+    probe.hierarchize()
+    cap = 3 * probe.device_bytes()
+    srv = sg.Server(cap, max_batch_points=1 << 16)
+    want = {}
+    for i, (d, n, fn, p) in enumerate(shapes):
+        g = sg.Grid(d, n)
+        g.sample_function(fn, p)
+        g.hierarchize()
+        X = inputs.uniform_points(300 + i, 4000, d)
+        want[i] = (X, g.evaluate(X))
+    for q in range(30):
+        i = (q * 7) % len(shapes)
+        d, n, fn, p = shapes[i]
+        gid = srv.add_grid(d, n, fn, p)
+        X, ref = want[i]
+        out, _ = srv.wait(srv.submit(gid, X))
+        assert np.array_equal(out.view(np.uint32), ref.view(np.uint32)), (q, shapes[i])
+        st = srv.stats()
+        assert st["bytes_in_use"] <= cap
+    assert srv.stats()["evictions"] > 0 and srv.stats()["failed"] == 0
+    srv.close()
