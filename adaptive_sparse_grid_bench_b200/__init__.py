@@ -9,6 +9,7 @@ from ._lib import (SG_HIER_FP32, SG_HIER_FP64, SG_OPT_EVAL_BLOCKS, SG_OPT_EVAL_P
                    header_functions, lib)
 from .batch import Batch  # noqa: F401
 from .grid import Grid  # noqa: F401
+from .refine import refine, refine_step  # noqa: F401
 from .server import Server  # noqa: F401
 
-__all__ = ["Grid", "Batch", "Server", "SgError", "lib", "header_functions"]
+__all__ = ["Grid", "Batch", "Server", "SgError", "lib", "header_functions", "refine", "refine_step"]

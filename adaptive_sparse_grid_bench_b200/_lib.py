@@ -80,6 +80,9 @@ SIGNATURES = {
     "sg_timings": (_i, [_p, _p]),
     "sg_kernel_launches": (_i, [_pi64]),
     "sg_sample_function": (_i, [_p, _i, _p, _i, _p]),
+    "sg_subspace_maxabs": (_i, [_p, _p]),
+    "sg_refine_step": (_i, [_i, _i, _p, _p, C.c_double, _i, _p, _p, _p]),
+    "sg_refine": (_i, [_i, _i, _p, _i, _p, _i, C.c_double, _i, _i64, _i, _i, C.POINTER(_p), _p]),
     "sg_batch_create": (_i, [_i, _p, _p, _p, C.POINTER(_p)]),
     "sg_batch_destroy": (_i, [_p]),
     "sg_batch_num_grids": (_i, [_p, _p]),

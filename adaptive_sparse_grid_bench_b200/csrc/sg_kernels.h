@@ -117,6 +117,10 @@ int sgk_gp2idx(const sg_layout *L, const int *levels, const int *indices, int64_
 int sgk_sample(const sg_layout *L, int fn, const double *params, int nparams, float *alpha,
                void *stream);
 
+/* out[q] = bits of max |alpha| over subspace q (subspaces in group order,
+ * positions as sg_layout_idx2l), alpha in the group-aligned layout. */
+int sgk_subspace_maxabs(const sg_layout *L, const float *alpha, unsigned *out, void *stream);
+
 int sgk_num_sms(void);
 
 /* Device address and size of the fixed no-allocation scratch array on the

@@ -687,6 +687,24 @@ SG_API int sg_evaluate(sg_grid *g, const float *coords, float *out, int64_t m)
     return r;
 }
 
+SG_API int sg_subspace_maxabs(sg_grid *g, float *maxabs)
+{
+    int prev, r;
+    cudaError_t e;
+    if (!g || !maxabs) return fail(SG_ERR_ARG, "sg_subspace_maxabs: NULL argument");
+    if (!g->has_values) return fail(SG_ERR_STATE, "sg_subspace_maxabs: no values have been set");
+    if ((r = enter(g, &prev)) != SG_OK) return r;
+    r = ensure(g, &g->d_scratch, &g->scratch_bytes, g->L.S * 4, "subspace statistics");
+    if (r == SG_OK) {
+        e = (cudaError_t)sgk_subspace_maxabs(&g->L, g->d_alpha, (unsigned *)g->d_scratch, 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(maxabs, g->d_scratch, (size_t)g->L.S * 4, cudaMemcpyDeviceToHost, 0);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+        if (e != cudaSuccess) r = cuda_fail(e, "sg_subspace_maxabs");
+    }
+    leave(g, prev);
+    return r;
+}
+
 SG_API int sg_sample_function(sg_grid *g, int fn, const double *params, int np, void *stream)
 {
     int prev, r, e, need = 0;

@@ -43,7 +43,22 @@ class Grid:
                 raise ValueError("limits must have num_dims entries")
             lim = _ptr(self._lim_buf)
         check(lib.sg_create(num_dims, num_levels, lim, C.byref(h)))
+        self._adopt(h)
+
+    @classmethod
+    def from_handle(cls, h: C.c_void_p) -> "Grid":
+        """Wraps an sg_grid handle made by the library (e.g. by sg_refine);
+        the Grid owns it from then on."""
+        g = cls.__new__(cls)
+        g._adopt(h)
+        return g
+
+    def _adopt(self, h: C.c_void_p) -> None:
+        lib = L.lib()
         self._h = h
+        d, n = C.c_int(), C.c_int()
+        check(lib.sg_dims(h, C.byref(d), C.byref(n), None))
+        num_dims, num_levels = d.value, n.value
         self.d = num_dims
         self.n = num_levels
         v = C.c_int64()
@@ -161,6 +176,12 @@ class Grid:
 
     def hierarchize(self) -> None:
         check(L.lib().sg_hierarchize(self._h))
+
+    def subspace_maxabs(self) -> np.ndarray:
+        """max |value| per subspace (compact subspace order), S floats."""
+        out = np.empty(self.num_subspaces, np.float32)
+        check(L.lib().sg_subspace_maxabs(self._h, _ptr(out)))
+        return out
 
     def evaluate(self, coord_mat) -> np.ndarray:
         X = np.ascontiguousarray(coord_mat, np.float32).reshape(-1, self.d)

@@ -43,14 +43,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--points", type=int, default=M_EVAL, help="query points per rank and step")
+    ap.add_argument("--points", type=int, default=None,
+                    help="query points per rank and step (default: the workload's, 2^24 for single)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per reference sample")
-    ap.add_argument("--workload", default="single", choices=["single", "batched", "served"],
-                    help="single: the d=10 n=10 grid (default); batched: many grids of mixed d and n; "
-                         "served: Poisson request stream against resident grids")
+    ap.add_argument("--workload", default="single", choices=["single", "adaptive", "batched", "served"],
+                    help="single: the d=10 n=10 grid (default); adaptive: the refined d=6 grid; batched: many "
+                         "grids of mixed d and n; served: Poisson request stream against resident grids")
     ap.add_argument("--grids", type=int, default=4096, help="batched: number of grids")
     ap.add_argument("--rates", default="1000,2000,4000,8000,16000", help="served: arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=3000, help="served: requests per rate")
@@ -110,13 +111,56 @@ class Clocks:
 
 
 # ---------------------------------------------------------------------------
-def reference_cpu(values: np.ndarray, X: np.ndarray, seconds: float):
+def single_workload():
+    """The d=10 n=10 regular grid of exp(-|x|^2) at 2^24 uniform points."""
+    from adaptive_sparse_grid_bench_b200 import Grid, inputs
+    from adaptive_sparse_grid_bench_b200._lib import SG_FN_GAUSS
+    return {"name": WORKLOAD, "d": D, "n": NLEV, "limits": None, "fn": SG_FN_GAUSS, "params": (),
+            "m_eval": M_EVAL, "make_grid": lambda: Grid(D, NLEV),
+            "points": lambda rank, m: inputs.uniform_points(SEED + rank, m, D),
+            "l2": "inputs larger than L2 (132 MB grid + 671 MB points)", "info": {}}
+
+
+def adaptive_workload(args):
+    """Limits-adaptive grid, d=6: from the regular level-4 grid, refine the
+    children of subspaces holding a surplus above 1e-4 up to level 13
+    (0-based) per dimension on exp(-50 |x - 0.3|^2), stopping before a grid
+    above the regular level-14 bound (109,051,905 points); evaluate 2^22
+    points, half uniform on [0,1)^6 and half N(0.3, 0.1^2) clipped to [0,1)
+    (seed 2)."""
+    from adaptive_sparse_grid_bench_b200 import inputs, refine
+    from adaptive_sparse_grid_bench_b200._lib import SG_FN_BUMP
+    d, m_eval, info = 6, 1 << 22, {}
+
+    def make_grid():
+        t0 = time.perf_counter()
+        g, it = refine(d, 4, SG_FN_BUMP, (0.3, 50.0), tol=1e-4, max_level=13, max_points=109_051_905, max_iters=32)
+        info.update({"refine_s": time.perf_counter() - t0, "grids_built": it, "n": g.n,
+                     "limits": [int(x) for x in g.limits]})
+        wl["n"], wl["limits"] = g.n, [int(x) for x in g.limits]
+        return g
+
+    def points(rank, m):
+        h = m // 2
+        return np.concatenate([inputs.uniform_points(2 + 100 * rank, h, d),
+                               inputs.gaussian_points(2 + 100 * rank, m - h, d, 0.3, 0.1, start=1 << 40)])
+
+    wl = {"name": "limits-adaptive grid d=6 from n=4, tol 1e-4, level <= 13, f=exp(-50|x-0.3|^2), "
+                  "evaluate 2^22 points (half uniform, half N(0.3,0.1) clipped)",
+          "d": d, "n": None, "limits": None, "fn": SG_FN_BUMP, "params": (0.3, 50.0), "m_eval": m_eval,
+          "make_grid": make_grid, "points": points, "l2": "points larger than L2", "info": info}
+    return wl
+
+
+def reference_cpu(values: np.ndarray, X: np.ndarray, seconds: float, wl=None):
     """Times the reference's own CPU path (oracle/_ref) on a bounded sample:
     omp_hierarchize3 over the whole grid, omp_evaluate5 over as many query
     points as fit in `seconds` (16K-point chunks: the SSE variant keeps the
     coordinates in a stack array).  Returns (per-step evals/s, info)."""
     from oracle.oracle import Reference
-    r = Reference(D, NLEV)
+    wl = wl or single_workload()
+    M_STEP = wl["m_eval"]
+    r = Reference(wl["d"], wl["n"], wl["limits"])
     r.set_values(values)
     t0 = time.perf_counter()
     r.hierarchize(9)
@@ -130,17 +174,19 @@ def reference_cpu(values: np.ndarray, X: np.ndarray, seconds: float):
     t0 = time.perf_counter()
     out = r.evaluate(X[:m], 7)
     t_e = time.perf_counter() - t0
-    per_step = t_h + t_e * (M_EVAL / m)
+    per_step = t_h + t_e * (M_STEP / m)
     info = {"cores": int(r.lib().ref_max_threads()), "t_hierarchize_s": t_h, "t_eval_sample_s": t_e,
             "sample_points": m, "ref_out": out, "surplus": r.values()}
-    return M_EVAL / per_step, info
+    return M_STEP / per_step, info
 
 
-def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsample: int = 192, ref_out=None):
+def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsample: int = 192, ref_out=None,
+                  wl=None):
     """Max/relative error of the GPU results against the FP64 oracle on a
     sample of query points (checker only)."""
     from oracle.oracle import Oracle
-    o = Oracle(D, NLEV)
+    wl = wl or single_workload()
+    o = Oracle(wl["d"], wl["n"], wl["limits"])
     s64 = o.hierarchize_f64(values.astype(np.float64))
     idx = np.linspace(0, X.shape[0] - 1, nsample).astype(np.int64)
     u64 = o.evaluate_f64(s64, X[idx])
@@ -161,10 +207,16 @@ def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsampl
 def run_reference_arm(args, rank: int):
     if rank != 0:
         return
+    if args.workload != "single":
+        # the other workloads carry the reference's CPU time in their own
+        # line (cpu_baseline / plain per-grid arms)
+        print(json.dumps({"impl": "reference", "workload": args.workload,
+                          "unavailable": "the reference arm times the default single-grid workload only"}))
+        return
     from adaptive_sparse_grid_bench_b200 import Grid, inputs
     g = Grid(D, NLEV)
     vals = inputs.grid_values(g, inputs.f_gauss)
-    X = inputs.uniform_points(SEED, min(args.points, 1 << 20), D)
+    X = inputs.uniform_points(SEED, min(args.points or M_EVAL, 1 << 20), D)
     vals_per = []
     info = None
     for it in range(args.warmup + args.steps):
@@ -186,30 +238,28 @@ def run_reference_arm(args, rank: int):
     print(json.dumps(line), flush=True)
 
 
-def device_inputs(g, rank, npts, torch, dev):
-    from adaptive_sparse_grid_bench_b200 import inputs
-    from adaptive_sparse_grid_bench_b200._lib import SG_FN_GAUSS
-    g.sample_function(SG_FN_GAUSS)
+def device_inputs(g, wl, rank, npts, torch, dev):
+    g.sample_function(wl["fn"], wl["params"])
     vals = torch.empty(g.num_points, dtype=torch.float32, device=dev)
     g.get_values_device(vals)
     torch.cuda.synchronize()
-    X = inputs.uniform_points(SEED + rank, npts, D)
-    return vals, X
+    return vals, wl["points"](rank, npts)
 
 
-def run_b200(args, rank: int, world: int, local_rank: int):
+def run_b200(args, rank: int, world: int, local_rank: int, wl=None):
     import torch
     import torch.distributed as dist
-    from adaptive_sparse_grid_bench_b200 import Grid
     from adaptive_sparse_grid_bench_b200._lib import SG_OPT_PROFILE
     from adaptive_sparse_grid_bench_b200.sharding import max_over_ranks
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    g = Grid(D, NLEV)
+    wl = wl or single_workload()
+    D = wl["d"]
+    g = wl["make_grid"]()
     g.precision = args.precision
     g.set_option(SG_OPT_PROFILE, 1)
-    vals_d, X = device_inputs(g, rank, args.points, torch, dev)
+    vals_d, X = device_inputs(g, wl, rank, args.points if args.points else wl["m_eval"], torch, dev)
     m = X.shape[0]
     X_d = torch.from_numpy(X).to(dev)
     out_d = torch.empty(m, dtype=torch.float32, device=dev)
@@ -304,9 +354,10 @@ def run_b200(args, rank: int, world: int, local_rank: int):
         "metric": "evals/s", "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64; values sampled on device)",
-        "config": {"workload": WORKLOAD, "points_per_step_per_rank": m, "d": D, "n": NLEV,
-                   "num_points": g.num_points, "num_subspaces": S, "hier_precision": args.precision,
-                   "l2": "inputs larger than L2 (132 MB grid + 671 MB points)", "parallelism": f"replicas x{world}"},
+        "config": {"workload": wl["name"], "points_per_step_per_rank": m, "d": D, "n": g.n,
+                   "limits": [int(x) for x in g.limits], "num_points": g.num_points, "num_subspaces": S,
+                   "hier_precision": args.precision, "l2": wl["l2"], "parallelism": f"replicas x{world}",
+                   **wl["info"]},
         "hierarchize": {"value": hier_gbs, "unit": "GB/s", "ms": hier_ms, "bytes": "8*d*N"},
         "evaluate": {"ms": eval_ms, "sort_ms": statistics.mean(t_sort), "evals_per_s": m / (eval_ms / 1e3),
                      "pairs_per_s": m * S / (eval_ms / 1e3)},
@@ -319,11 +370,12 @@ def run_b200(args, rank: int, world: int, local_rank: int):
     }
     if world == 1 and not args.no_cpu_baseline:
         vals = vals_d.cpu().numpy()
-        cpu_v, info = reference_cpu(vals, X, args.cpu_seconds)
+        cpu_v, info = reference_cpu(vals, X, args.cpu_seconds, wl)
         line["cpu_baseline"] = {"value": cpu_v, "unit": "evals/s", "cores": info["cores"], "kind": "reference",
                                 "sample": (f"reference omp_hierarchize3 on the full grid + omp_evaluate5 on "
-                                           f"{info['sample_points']} of 2^24 points, extrapolated linearly")}
-        line["err_vs_fp64"] = error_vs_fp64(vals, out_d.cpu().numpy(), X, ref_out=info["ref_out"])
+                                           f"{info['sample_points']} of {wl['m_eval']} points, extrapolated "
+                                           f"linearly")}
+        line["err_vs_fp64"] = error_vs_fp64(vals, out_d.cpu().numpy(), X, ref_out=info["ref_out"], wl=wl)
     print(json.dumps(line), flush=True)
 
 
@@ -628,6 +680,8 @@ def main():
             run_batched(args, rank, world, local_rank)
         elif args.workload == "served":
             run_served(args, rank, world, local_rank)
+        elif args.workload == "adaptive":
+            run_b200(args, rank, world, local_rank, adaptive_workload(args))
         else:
             run_b200(args, rank, world, local_rank)
     finally:

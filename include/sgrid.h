@@ -160,6 +160,31 @@ int sg_gp2idx_device(const sg_grid *grid, const int *levels, const int *indices,
  * array like sg_set_values). */
 int sg_sample_function(sg_grid *grid, int fn, const double *params, int num_params, void *stream);
 
+/* ---- limits-adaptive refinement -----------------------------------------
+ * The reference's adaptive grid is the per-dimension limit vector of
+ * init() (c:82-83, c:113-129) and nothing refines it.  These calls refine
+ * within that family, so every grid they produce is one the reference's
+ * init/idx2gp/hierarchize0 reproduce for the same (d, n, limits).
+ * Levels are 0-based as in the reference. */
+/* maxabs[q] = max |value| over the points of subspace q (subspaces in
+ * compact order: level sum s ascending, sg_idx2l positions inside a group);
+ * S floats.  Runs on the legacy default stream and waits for it. */
+int sg_subspace_maxabs(sg_grid *grid, float *maxabs);
+/* One step: a subspace is active if maxabs > tol; every child l + e_k with
+ * l_k < max_level of an active subspace must be in the next grid, which is
+ * the smallest (n_out, limits_out) containing (n, limits) and those
+ * children (n_out capped at SG_MAX_LEVELS).  changed = 0 when it is the
+ * same grid.  Host only. */
+int sg_refine_step(int d, int n, const int *limits, const float *maxabs, double tol, int max_level,
+                   int *n_out, int *limits_out, int *changed);
+/* Driver: from (d, n0, limits0 or NULL), sample fn, hierarchize (precision
+ * SG_HIER_FP32/FP64), measure, step, until the grid stops changing, after
+ * max_iters grids, or before a grid of more than max_points points.
+ * Returns the last grid, hierarchized; sg_dims reads its n and limits. */
+int sg_refine(int d, int n0, const int *limits0, int fn, const double *params, int num_params, double tol,
+              int max_level, int64_t max_points, int max_iters, int precision, sg_grid **grid,
+              int *iterations);
+
 /* ---- batches of independent grids -------------------------------------
  * Many grids of mixed d, n and limits held in one device buffer and run
  * through a fixed set of launches (replayed as one CUDA graph).  No
