@@ -19,7 +19,8 @@ int eval_launch(const EvalArgs &A, int ppt, void *stream);
 /* Points per CTA of the evaluation kernels for `ppt` points per thread. */
 #define SG_EVAL_CTA_POINTS(ppt) (256 * (ppt))
 
-/* Batched form: items[b] = (grid index into `grids`, first point) for CTA b;
+/* Batched form: items[b] = (grid index into `grids` | part << 29, first
+ * point) for CTA b;
  * every grid of the launch has dimension D. */
 template <int D>
 int eval_batch_launch(const EvalArgs *grids, const int2 *items, int nitems, int ppt, void *stream);

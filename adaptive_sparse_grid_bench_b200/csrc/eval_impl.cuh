@@ -21,10 +21,12 @@
  *   - 2^b - 1 + t_b and the hats of dims A, B (and C for small budgets) are
  *     precomputed per point in registers, so each subspace costs one add,
  *     one gather and one FMA;
- *   - in regular grids, blocks of budget R <= kRF run fully unrolled; larger
- *     blocks loop over their planes and run each plane's 2-D sub-block fully
- *     unrolled behind a jump table; a generic loop covers limits on the
- *     innermost dims, budgets >= kNB and d = 1;
+ *   - blocks of budget R <= kRF run fully unrolled; larger blocks loop over
+ *     their planes and run each plane's 2-D sub-block fully unrolled behind a
+ *     jump table.  A block or sub-block whose budget is within the limits of
+ *     its dims has the regular shape whatever the limits, so limit-vector
+ *     (adaptive) grids take the unrolled code too; a generic loop covers
+ *     budgets above the limits, budgets >= kNB and d = 1;
  *   - per prefix dim the walk keeps three values per point: the fractional
  *     part y = frac(x 2^l) (next level: doubling, exact in FP32), the cell
  *     index of the prefix (next level: 2*ix + bit) and the parent's product;
@@ -83,7 +85,7 @@ struct Inner {
     uint32_t TC[P];       /* floor(x_C 2^15)                         */
 };
 
-/* Regular-grid shapes (all innermost limits >= n-1). */
+/* Regular shapes: blocks whose budget is within the innermost limits. */
 __host__ __device__ constexpr uint32_t plen_reg(int r, int a) { return (2u << (r - a)) - 1u; }
 __host__ __device__ constexpr uint32_t aoff_reg(int r, int a)
 {
@@ -186,12 +188,12 @@ __device__ __forceinline__ void block2_generic(const float *__restrict__ alpha, 
     }
 }
 
-/* Sub-block of budget r: unrolled (regular, r < kNB) or generic. */
+/* Sub-block of budget r: unrolled (r within the limits, r < kNB) or generic. */
 template <int D, int P>
 __device__ __forceinline__ void block2_any(const EvalArgs &A, int r, const Inner<P> &in, const float (&xA)[P],
                                            const float (&xB)[P], const uint32_t (&base)[P], float (&s)[P])
 {
-    if (D >= 2 && A.regular) {
+    if (D >= 2 && r <= A.lim2) {
         switch (r) {
 #define SG_BLK2(RR) \
     case RR: block2_fixed<RR, P>(A.alpha, base, in, s); return;
@@ -211,7 +213,7 @@ __device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<
                                           float (&s)[P])
 {
     if constexpr (D >= 3) {
-        if (A.regular && R <= kRF) {
+        if (R <= kRF && R <= A.lim3) {
             switch (R) {
             case 0: block3_planes<0, 0, P>(A.alpha, base, in, s); return;
             case 1: block3_planes<1, 0, P>(A.alpha, base, in, s); return;
@@ -248,11 +250,19 @@ __device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<
     }
 }
 
-/* Walk over prefix dim K (K <= D-4); children of depth D-4 are blocks. */
-template <int D, int K, int P>
+/* The walk's block range of a split evaluation: blocks are numbered in
+ * walk order; only [lo, hi) are summed (all of them when !partial). */
+struct Range {
+    uint32_t leaf, lo, hi;
+    bool partial;
+};
+
+/* Walk over prefix dim K (K <= D-4); children of depth D-4 are blocks.
+ * SPLIT: the caller may ask for a block range (batched launches). */
+template <int D, int K, int P, bool SPLIT>
 struct Walk {
     static __device__ __forceinline__ void run(const EvalArgs &A, const float *sx, int tid, int budget,
-                                               uint32_t &cur, const Inner<P> &in, const float (&xC)[P],
+                                               uint32_t &cur, Range &rg, const Inner<P> &in, const float (&xC)[P],
                                                const float (&xA)[P], const float (&xB)[P], const float (&pin)[P],
                                                const uint32_t (&ixin)[P], float (&sum)[P], float (&comp)[P])
     {
@@ -270,6 +280,17 @@ struct Walk {
 #pragma unroll
                 for (int p = 0; p < P; ++p) ix[p] = 2 * ix[p] + step_y(y[p]);
             }
+            if (SPLIT && rg.partial) {
+                /* the child subtree (depth K+1, budget - l) holds blocks
+                 * [leaf, leaf + nb): skip it whole when outside [lo, hi) */
+                const uint32_t *w = A.walk + 2 * ((K + 1) * (A.nm1 + 1) + (budget - l));
+                const uint32_t nb = __ldg(w);
+                if (rg.leaf + nb <= rg.lo || rg.leaf >= rg.hi) {
+                    rg.leaf += nb;
+                    cur += __ldg(w + 1);
+                    continue;
+                }
+            }
             float pn[P];
 #pragma unroll
             for (int p = 0; p < P; ++p) pn[p] = pin[p] * hat_of(y[p]);
@@ -281,11 +302,12 @@ struct Walk {
 #pragma unroll
                 for (int p = 0; p < P; ++p) base[p] = cur + ix[p] * blk;
                 cur += blk << (A.nm1 - R);
+                if (SPLIT) ++rg.leaf;
                 block_sum<D, P>(A, R, in, xC, xA, xB, base, s);
 #pragma unroll
                 for (int p = 0; p < P; ++p) acc[p] = fmaf(pn[p], s[p], acc[p]);
             } else {
-                Walk<D, K + 1, P>::run(A, sx, tid, budget - l, cur, in, xC, xA, xB, pn, ix, sum, comp);
+                Walk<D, K + 1, P, SPLIT>::run(A, sx, tid, budget - l, cur, rg, in, xC, xA, xB, pn, ix, sum, comp);
             }
         }
         if constexpr (K == D - 4) {
@@ -298,8 +320,9 @@ struct Walk {
 /* Evaluates this thread's points first, first + 32, ..., first + 32(P-1)
  * (those below `end`) against grid A; sx is this CTA's shared coordinate
  * buffer. */
-template <int D, int P>
-__device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int tid, int64_t first, int64_t end)
+template <int D, int P, bool SPLIT>
+__device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int tid, int64_t first, int64_t end,
+                                            int part)
 {
 
     float xC[P], xA[P], xB[P];
@@ -374,7 +397,12 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int ti
             pin[p] = 1.0f;
             ix[p] = 0;
         }
-        Walk<D, 0, P>::run(A, sx, tid, A.nm1, cur, in, xC, xA, xB, pin, ix, sum, comp);
+        Range rg;
+        rg.leaf = 0;
+        rg.partial = SPLIT && A.nparts > 1;
+        rg.lo = rg.partial ? A.split[part] : 0u;
+        rg.hi = rg.partial ? A.split[part + 1] : 0xFFFFFFFFu;
+        Walk<D, 0, P, SPLIT>::run(A, sx, tid, A.nm1, cur, rg, in, xC, xA, xB, pin, ix, sum, comp);
     } else {
         uint32_t base[P];
         float s[P];
@@ -390,7 +418,10 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int ti
         const int64_t i = first + 32 * p;
         if (i < end) {
             const float r = valid[p] ? __fsub_rn(sum[p], comp[p]) : (nan_in[p] ? __int_as_float(0x7fc00000) : 0.0f);
-            A.out[A.perm ? A.perm[i] : i] = r;
+            if (SPLIT && A.nparts > 1)
+                A.part_out[(int64_t)part * A.num_evals + i] = r;
+            else
+                A.out[A.perm ? A.perm[i] : i] = r;
         }
     }
 }
@@ -402,11 +433,12 @@ __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const E
     __shared__ float sx[NPX * P * kThreads];
     const int tid = threadIdx.x;
     const int64_t warp = (blockIdx.x * (int64_t)kThreads + tid) >> 5;
-    eval_points<D, P>(A, sx, tid, warp * (32 * P) + (tid & 31), A.num_evals);
+    eval_points<D, P, false>(A, sx, tid, warp * (32 * P) + (tid & 31), A.num_evals, 0);
 }
 
 /* Many grids of the same dimension in one launch: CTA b evaluates the
- * kThreads*P points of grid items[b].x starting at point items[b].y. */
+ * kThreads*P points of grid items[b].x & (2^29-1) starting at point
+ * items[b].y; bits 29..31 of items[b].x select the part of a split sum. */
 template <int D, int P>
 __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3))
     k_evaluate_batch(const EvalArgs *__restrict__ grids, const int2 *__restrict__ items)
@@ -416,15 +448,16 @@ __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3))
     __shared__ EvalArgs sA;
     const int tid = threadIdx.x;
     const int2 item = items[blockIdx.x];
+    const int q = item.x & 0x1FFFFFFF, part = (int)((unsigned)item.x >> 29); /* grid, part of a split sum */
     {
-        const uint32_t *src = reinterpret_cast<const uint32_t *>(grids + item.x);
+        const uint32_t *src = reinterpret_cast<const uint32_t *>(grids + q);
         uint32_t *dst = reinterpret_cast<uint32_t *>(&sA);
         for (int w = tid; w < (int)(sizeof(EvalArgs) / 4); w += kThreads) dst[w] = src[w];
     }
     __syncthreads();
     const int64_t start = item.y;
     const int64_t end = min(start + (int64_t)kThreads * P, sA.num_evals);
-    eval_points<D, P>(sA, sx, tid, start + (tid >> 5) * (32 * P) + (tid & 31), end);
+    eval_points<D, P, true>(sA, sx, tid, start + (tid >> 5) * (32 * P) + (tid & 31), end, part);
 }
 
 template <int D, int P>

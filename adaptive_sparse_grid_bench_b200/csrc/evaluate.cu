@@ -1,33 +1,16 @@
 /*
- * Evaluation kernels for sm_100a.
+ * Evaluation support on sm_100a: the compact -> block layout repack, the
+ * spatial (Morton) ordering of query points, and the launchers of the
+ * evaluation kernels.  The kernels themselves (one instantiation per d,
+ * eval_d*.cu) are in eval_impl.cuh, which describes the walk; reference
+ * algorithm: evaluate0 in adaptive_sparse_grid_bench.c:1237-1274 and
+ * evaluate5 (c:1558-1688).
  *
- * Reference algorithm: evaluate0 in adaptive_sparse_grid_bench.c:1237-1274
- * (definition) and evaluate5 (c:1558-1688): for a query point x,
- *     u(x) = sum over subspaces l of  a[off(l) + idx(x, l)] * prod_k hat_k
- * with t_k = floor(x_k 2^l_k), idx(x, l) = row-major (t_0, ..., t_{d-1}) over
- * the subspace (dim 0 most significant) and hat_k = 1 - |x_k 2^(l_k+1) - (2t_k+1)|.
- *
- * B200 design.  One thread owns PPT query points; every warp walks the same
- * depth-first tree over the level vectors of the prefix dims 0..d-3 (each
- * dim's level ascending, sum(l) <= n-1, l_k <= limits[k]), so control flow is
- * uniform across the warp and partial products / partial cell indices are
- * shared by all subspaces below a node.  At depth d-2 the walk reaches a
- * block: every subspace of the two innermost dims (A = d-2, B = d-1) under
- * that prefix, stored contiguously per prefix cell in the block layout (see
- * sg_layout.h), with dim B's levels as a 1-D heap.  The surplus of (a, b) is
- * then at base + aoff(a) + t_a*plen(a) + (2^b - 1 + t_b):
- *   - base is one multiply-add per block and point; the row offset one
- *     multiply-add per row; 2^b - 1 + t_b and the hats of dims A and B are
- *     precomputed per point in registers, so each subspace costs one add,
- *     one gather and one FMA;
- *   - blocks of budget R < 12 (all of them in regular grids up to n = 12)
- *     run fully unrolled, so a block's gathers issue back to back;
- *   - hats of the prefix dims come from the previous level's with a doubling
- *     (exact in FP32), so no division or table appears in the walk;
- *   - each block's partial sum enters a Kahan-compensated accumulator.
- * Query points are first put in spatial (Morton) order on the GPU so that
- * the 32 points of a warp land in few cells of each subspace: the gathers
- * then touch few sectors and the grid is served from L1/L2.
+ * Query points are put in Morton order on the GPU first (counting sort over
+ * 2^20 cells: keys, a three-level scan, a stable scatter), so the 32 points
+ * of a warp land in few cells of each subspace: their gathers touch few
+ * sectors and the grid is served from L1/L2.  Results are scattered back to
+ * the caller's order by the permutation.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -38,6 +21,27 @@
 namespace {
 
 constexpr int kThreads = 256;
+
+/* Adds the parts of split sums in part order with Kahan compensation; CTA
+ * b covers kThreads points of request items[b].x from point items[b].y. */
+__global__ void __launch_bounds__(kThreads) k_combine_parts(const sg_eval_args *__restrict__ grids,
+                                                            const int2 *__restrict__ items)
+{
+    const int2 item = items[blockIdx.x];
+    const sg_eval_args *A = grids + item.x;
+    const int64_t m = A->num_evals, i = (int64_t)item.y + threadIdx.x;
+    if (i >= m) return;
+    const int np = A->nparts;
+    const float *src = A->part_out;
+    float s = 0.0f, c = 0.0f;
+    for (int k = 0; k < np; ++k) {
+        const float y = __fsub_rn(src[k * m + i], c);
+        const float t = __fadd_rn(s, y);
+        c = __fsub_rn(__fsub_rn(t, s), y);
+        s = t;
+    }
+    A->out[i] = __fsub_rn(s, c);
+}
 
 /* compact (group-aligned) layout -> block layout, one CTA per subspace */
 __global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
@@ -203,9 +207,13 @@ void sgk_fill_eval_args(const sg_eval_plan *p, const float *coords, const int32_
         A->blk3[r] = p->blk3[r];
         A->blk2[r] = p->blk2[r];
     }
-    bool reg = true;
-    for (int k = p->d >= 3 ? p->d - 3 : 0; k < p->d; ++k) reg = reg && p->lim[k] >= p->n - 1;
-    A->regular = reg;
+    const int la = p->d >= 2 ? p->lim[p->d - 2] : 0, lb = p->lim[p->d - 1], lc = p->d >= 3 ? p->lim[p->d - 3] : 0;
+    A->lim2 = p->d >= 2 ? (la < lb ? la : lb) : 0;
+    A->lim3 = p->d >= 3 ? (lc < A->lim2 ? lc : A->lim2) : 0;
+    A->nparts = 1;
+    for (int k = 0; k <= SG_EVAL_MAX_PARTS; ++k) A->split[k] = k ? 0xFFFFFFFFu : 0u;
+    A->part_out = NULL;
+    A->walk = NULL;
 }
 
 int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
@@ -238,6 +246,14 @@ int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, i
 #undef SG_D
     default: return cudaErrorInvalidValue;
     }
+}
+
+int sgk_combine_parts(const sg_eval_args *grids, const int32_t *items, int nitems, void *stream)
+{
+    if (nitems <= 0) return cudaSuccess;
+    k_combine_parts<<<nitems, kThreads, 0, (cudaStream_t)stream>>>(grids, reinterpret_cast<const int2 *>(items));
+    sgk_count(1);
+    return cudaGetLastError();
 }
 
 int sgk_repack(const float *src, float *dst, const sg_repack *rp, int64_t nsub, void *stream)

@@ -42,6 +42,9 @@ struct sg_grid {
     int64_t dev_bytes;
     cudaEvent_t ev[SG_NUM_PHASES][2]; /* profiling: start/stop per phase */
     int ev_used[SG_NUM_PHASES];
+    uint32_t *d_walk;    /* evaluation walk tables (split sums only)     */
+    int nparts;          /* parts of a split sum in batched launches (0/1: whole) */
+    uint32_t split[SG_EVAL_MAX_PARTS + 1];
     sg_dev_alloc_fn alloc; /* NULL: cudaMalloc/cudaFree */
     sg_dev_free_fn free_fn;
     void *alloc_ctx;
@@ -54,7 +57,12 @@ int sg_create_with_allocator(int d, int n, const int *limits, sg_dev_alloc_fn al
 
 /* Builds the block layout if the values changed since it was last built. */
 int sg_grid_prepare_eval(sg_grid *g, cudaStream_t st);
-/* Kernel arguments to evaluate grid g at m points (device pointers). */
+/* Splits each point's sum over the subspaces into nparts block ranges of
+ * about equal work for batched evaluations (d >= 4; otherwise, or for
+ * nparts <= 1, whole sums).  Uploads the walk tables on st. */
+int sg_grid_set_parts(sg_grid *g, int nparts, cudaStream_t st);
+/* Kernel arguments to evaluate grid g at m points (device pointers); a
+ * split grid's arguments carry its parts, part_out is left to the caller. */
 void sg_grid_eval_args(const sg_grid *g, const float *coords, float *out, int64_t m, sg_eval_args *a);
 
 #endif

@@ -56,6 +56,11 @@ typedef struct sg_eval_plan {
     int ppt;                     /* points per thread (1 or 2)               */
 } sg_eval_plan;
 
+/* A point's sum over the subspaces can be split into up to this many
+ * parts (ranges of the walk's blocks), evaluated by separate CTAs and added
+ * in part order afterwards: bounds the latency of one point on a large grid. */
+#define SG_EVAL_MAX_PARTS 8
+
 /* Per-grid arguments of the evaluation kernels (also the element type of
  * the batched launch's grid table). */
 typedef struct sg_eval_args {
@@ -65,10 +70,21 @@ typedef struct sg_eval_args {
     float *out;
     int64_t num_evals;
     int nm1;                 /* n - 1                                */
-    int regular;             /* innermost dims unrestricted          */
+    int lim2;                /* min limit of dims d-2, d-1: a sub-block of
+                                budget r <= lim2 has the regular shape  */
+    int lim3;                /* min limit of dims d-3..d-1 (3-D blocks) */
     int lim[SG_MAX_DIMS];
     uint32_t blk3[SG_MAX_LEVELS]; /* block size per budget R         */
     uint32_t blk2[SG_MAX_LEVELS]; /* sub-block size per budget r     */
+    /* split evaluation (batched launch only; nparts 1 = whole sums):
+     * part k covers the walk's blocks [split[k], split[k+1]) and writes its
+     * sums to part_out[k * num_evals + i]; walk = per (prefix depth K,
+     * budget b) the block count and block-layout extent of the subtree
+     * (sg_layout_walk_tables), used to skip subtrees outside the range. */
+    int nparts;
+    uint32_t split[SG_EVAL_MAX_PARTS + 1];
+    float *part_out;
+    const uint32_t *walk;
 } sg_eval_args;
 
 void sgk_fill_eval_args(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
@@ -78,10 +94,16 @@ void sgk_fill_eval_args(const sg_eval_plan *p, const float *coords, const int32_
 int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
                  int64_t num_evals, void *stream);
 /* Many grids of dimension d in one launch: items (device, 2 ints per CTA) =
- * (index into grids, first point); each CTA covers SG_EVAL_CTA_POINTS(ppt)
- * points of its grid. */
+ * (index into grids | part << 29, first point); each CTA covers
+ * SG_EVAL_CTA_POINTS(ppt) points of its grid (index < 2^29; part selects
+ * the block range of a split sum, 0 for whole sums). */
 int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, int nitems, int ppt,
                        void *stream);
+
+/* out[i] = compensated sum over k < nparts of part_out[k * num_evals + i]
+ * (part order) for the split grids: items as for sgk_evaluate_batch, one
+ * CTA per 256 points. */
+int sgk_combine_parts(const sg_eval_args *grids, const int32_t *items, int nitems, void *stream);
 
 /* Reorders the surpluses from the group-aligned compact layout into the
  * block layout (one descriptor per subspace). */

@@ -317,3 +317,98 @@ int sg_layout_eval_tables(const sg_layout *L, sg_repack **repack, uint32_t *blk3
     *repack = rp;
     return SG_OK;
 }
+
+/* ---- walk tables and split evaluation ----------------------------------- */
+
+int sg_layout_walk_tables(const sg_layout *L, const uint32_t *blk3, uint32_t *walk)
+{
+    const int d = L->d, n = L->n;
+    int K, b, l;
+    if (d < 4) return SG_ERR_ARG;
+    for (b = 0; b < n; b++) {
+        walk[2 * ((d - 3) * n + b)] = 1;
+        walk[2 * ((d - 3) * n + b) + 1] = blk3[b] << (n - 1 - b);
+    }
+    for (K = d - 4; K >= 0; K--)
+        for (b = 0; b < n; b++) {
+            uint64_t cnt = 0, ext = 0;
+            for (l = 0; l <= b && l <= L->lim[K]; l++) {
+                cnt += walk[2 * ((K + 1) * n + b - l)];
+                ext += walk[2 * ((K + 1) * n + b - l) + 1];
+            }
+            walk[2 * (K * n + b)] = (uint32_t)cnt;
+            walk[2 * (K * n + b) + 1] = (uint32_t)ext;
+        }
+    return SG_OK;
+}
+
+/* subspaces (c, a, b) of the innermost dims with c + a + b <= R, in limits */
+static double block_subspaces(const sg_layout *L, int R)
+{
+    const int lc = L->lim[L->d - 3], la = L->lim[L->d - 2], lb = L->lim[L->d - 1];
+    double cnt = 0.0;
+    int c, a;
+    for (c = 0; c <= R && c <= lc; c++)
+        for (a = 0; a <= R - c && a <= la; a++) cnt += (R - c - a < lb ? R - c - a : lb) + 1;
+    return cnt;
+}
+
+#define SG_BLOCK_OVERHEAD 3.0 /* per-block walk cost in subspace-equivalents */
+
+int sg_layout_walk_split(const sg_layout *L, int nparts, uint32_t *bounds)
+{
+    const int d = L->d, n = L->n;
+    double *W;
+    uint32_t *cnt;
+    int K, b, l, j;
+    if (d < 4 || nparts < 1) return SG_ERR_ARG;
+    W = (double *)malloc(sizeof(double) * (size_t)(d - 2) * (size_t)n);
+    cnt = (uint32_t *)malloc(sizeof(uint32_t) * (size_t)(d - 2) * (size_t)n);
+    if (!W || !cnt) {
+        free(W);
+        free(cnt);
+        return SG_ERR_NOMEM;
+    }
+    for (b = 0; b < n; b++) {
+        W[(d - 3) * n + b] = block_subspaces(L, b) + SG_BLOCK_OVERHEAD;
+        cnt[(d - 3) * n + b] = 1;
+    }
+    for (K = d - 4; K >= 0; K--)
+        for (b = 0; b < n; b++) {
+            double w = 0.0;
+            uint64_t c = 0;
+            for (l = 0; l <= b && l <= L->lim[K]; l++) {
+                w += W[(K + 1) * n + b - l];
+                c += cnt[(K + 1) * n + b - l];
+            }
+            W[K * n + b] = w;
+            cnt[K * n + b] = (uint32_t)c;
+        }
+    bounds[0] = 0;
+    bounds[nparts] = cnt[n - 1];
+    for (j = 1; j < nparts; j++) {
+        /* descend to the block holding work position j/nparts of the total */
+        const double t = W[n - 1] * j / nparts;
+        double acc = 0.0;
+        uint32_t leaf = 0;
+        K = 0;
+        b = n - 1;
+        while (K < d - 3) {
+            const int lmax = b < L->lim[K] ? b : L->lim[K];
+            for (l = 0; l <= lmax; l++) {
+                const double w = W[(K + 1) * n + b - l];
+                if (acc + w > t) break;
+                acc += w;
+                leaf += cnt[(K + 1) * n + b - l];
+            }
+            if (l > lmax) break; /* rounding: t at the very end */
+            K++;
+            b -= l;
+        }
+        bounds[j] = leaf < bounds[j - 1] ? bounds[j - 1] : leaf;
+        if (bounds[j] > bounds[nparts]) bounds[j] = bounds[nparts];
+    }
+    free(W);
+    free(cnt);
+    return SG_OK;
+}

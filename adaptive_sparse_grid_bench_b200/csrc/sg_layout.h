@@ -87,6 +87,16 @@ typedef struct sg_eval_shape {
 void sg_layout_eval_sub(const sg_layout *L, int r, sg_eval_sub *sh);
 void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh);
 
+/* Walk tables of the evaluation (d >= 4; the walk visits prefix dims
+ * 0..d-4, blocks sit at depth d-3).  For depth K = 0..d-3 and budget
+ * b = 0..n-1: walk[2*(K*n + b)] = number of blocks of the subtree entered at
+ * depth K with budget b, walk[2*(K*n + b) + 1] = their extent in the block
+ * layout (sum of blk3[R] << (n-1-R)).  walk has 2*(d-2)*n entries. */
+int sg_layout_walk_tables(const sg_layout *L, const uint32_t *blk3, uint32_t *walk);
+/* bounds[0..nparts]: block ranges of the walk with about equal work each
+ * (subspaces per block plus a per-block overhead); d >= 4. */
+int sg_layout_walk_split(const sg_layout *L, int nparts, uint32_t *bounds);
+
 /* Per-subspace repack descriptor (compact layout -> block layout). */
 typedef struct sg_repack {
     uint32_t src;  /* device offset of the subspace in the group-aligned layout */

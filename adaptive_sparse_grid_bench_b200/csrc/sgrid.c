@@ -101,6 +101,7 @@ static void free_device(sg_grid *g)
     dev_free(g, g->d_err);
     dev_free(g, g->d_scratch);
     dev_free(g, g->d_io);
+    dev_free(g, g->d_walk);
 }
 
 int sg_create_with_allocator(int d, int n, const int *limits, sg_dev_alloc_fn alloc, sg_dev_free_fn free_fn,
@@ -343,6 +344,7 @@ bad:
     g->d_blk = NULL;
     g->d_repack = NULL;
     g->d_err = NULL;
+    g->d_walk = NULL;
     g->d_scratch = g->d_io = NULL;
     g->scratch_bytes = g->io_bytes = g->dev_bytes = 0;
     g->dev = -1;
@@ -812,6 +814,35 @@ int sg_grid_prepare_eval(sg_grid *g, cudaStream_t st)
     return SG_OK;
 }
 
+int sg_grid_set_parts(sg_grid *g, int nparts, cudaStream_t st)
+{
+    const sg_layout *L = &g->L;
+    uint32_t *tab;
+    int64_t words;
+    int r;
+    cudaError_t e;
+    if (nparts > SG_EVAL_MAX_PARTS) nparts = SG_EVAL_MAX_PARTS;
+    if (L->d < 4 || nparts <= 1 || g->dev < 0) {
+        g->nparts = 1;
+        return SG_OK;
+    }
+    words = 2 * (int64_t)(L->d - 2) * L->n;
+    tab = (uint32_t *)malloc((size_t)words * sizeof(uint32_t));
+    if (!tab) return fail(SG_ERR_NOMEM, "sg_grid_set_parts: out of host memory");
+    r = sg_layout_walk_tables(L, g->blk3, tab);
+    if (r == SG_OK) r = sg_layout_walk_split(L, nparts, g->split);
+    if (r == SG_OK && !g->d_walk) r = dev_alloc(g, (void **)&g->d_walk, words * 4, "walk tables");
+    if (r == SG_OK) {
+        /* pageable source: the copy has taken the bytes when the call returns */
+        e = cudaMemcpyAsync(g->d_walk, tab, (size_t)words * 4, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) r = cuda_fail(e, "uploading the walk tables");
+    }
+    free(tab);
+    if (r != SG_OK) return r;
+    g->nparts = nparts;
+    return SG_OK;
+}
+
 void sg_grid_eval_args(const sg_grid *g, const float *coords, float *out, int64_t m, sg_eval_args *a)
 {
     sg_eval_plan p;
@@ -826,4 +857,9 @@ void sg_grid_eval_args(const sg_grid *g, const float *coords, float *out, int64_
     }
     p.ppt = 2;
     sgk_fill_eval_args(&p, coords, NULL, out, m, a);
+    if (g->nparts > 1) {
+        a->nparts = g->nparts;
+        for (k = 0; k <= g->nparts; k++) a->split[k] = g->split[k];
+        a->walk = g->d_walk;
+    }
 }

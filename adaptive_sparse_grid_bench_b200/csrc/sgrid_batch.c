@@ -53,7 +53,8 @@ SG_API int sg_batch_create(int num_grids, const int *dims, const int *levels, co
     sg_batch *b;
     int g, r;
     int64_t lim_at = 0, doff = 0, voff = 0;
-    if (!out || num_grids < 1 || !dims || !levels) return bfail(SG_ERR_ARG, "sg_batch_create: bad argument");
+    if (!out || num_grids < 1 || num_grids >= (1 << 29) || !dims || !levels)
+        return bfail(SG_ERR_ARG, "sg_batch_create: bad argument");
     *out = NULL;
     b = (sg_batch *)calloc(1, sizeof(sg_batch));
     if (!b) return bfail(SG_ERR_NOMEM, "sg_batch_create: out of host memory");

@@ -19,11 +19,22 @@
  * into one batch: one host->device copy of all their coordinates, one
  * batched evaluation launch per dimension present (the batched kernel treats
  * each request as a grid of its own), one device->host copy of the results.
- * Batches alternate between two slots with their own streams, so a batch is
- * assembled and copied while the previous one computes; requests that arrive
- * while a batch runs go into the next one as soon as a slot frees up.  A
- * request's result depends only on its grid and points, so it is the same
- * alone and in any mix.
+ * The per-dimension launches of a batch run concurrently on streams of their
+ * own (forked from and joined back to the slot's stream), so their tails
+ * overlap; inside a launch the CTAs of the grids with the most subspaces
+ * come first (longest first).  One point's sum over a grid's subspaces is
+ * a serial chain of work for one thread; on grids with many subspaces it is
+ * split into parts (block ranges of the evaluation walk, fixed per grid at
+ * admission), evaluated by separate CTAs and added in part order by a
+ * combine launch, and launches that still hold long chains use one point
+ * per thread: this bounds the latency of a request on a large grid.
+ * Batches alternate between two slots, so a batch is staged and copied
+ * while the previous one computes; requests that arrive while a batch runs
+ * go into the next one as soon as a slot frees up.  Staging (coordinates
+ * into pinned memory) and delivery (results into the callers' buffers) run
+ * outside the server lock.  A request's result depends only on its grid
+ * and points (the kernel's arithmetic for a point does not depend on the
+ * CTA shape), so it is the same alone and in any mix.
  */
 #include <cuda_runtime_api.h>
 #include <pthread.h>
@@ -39,7 +50,10 @@
 #define SG_API __attribute__((visibility("default")))
 #define SRV_SLOTS 2
 #define SRV_MAX_REQS 8192 /* requests per batch */
-#define SG_SERVER_CTA_POINTS 512 /* points per CTA of the batched kernel at 2 per thread */
+#define SRV_CTA_THREADS 256
+#define SRV_SPLIT_SUBSPACES 4096  /* grids (d >= 4) with this many subspaces get split sums */
+#define SRV_PART_SUBSPACES 2048   /* about this many subspaces per part (at most 8 parts) */
+#define SRV_LONG_CHAIN 2048       /* launches with a part this long use 1 point per thread */
 
 #define ARENA_ALIGN 256
 
@@ -171,18 +185,24 @@ typedef struct srv_req {
     int64_t m;
     double t_submit, t_done;
     int state; /* 0 queued, 1 running, 2 done, 3 failed */
+    int64_t S;  /* subspaces of the grid (set when batched) */
+    sg_grid *g; /* the grid (set when batched) */
     struct srv_req *next;
 } srv_req;
 
 typedef struct srv_slot {
     cudaStream_t st;
-    cudaEvent_t done;
+    cudaStream_t dst[SG_MAX_DIMS + 1]; /* per dimension: the batch's launches overlap */
+    cudaEvent_t done, ev_in, ev_d[SG_MAX_DIMS + 1];
     int busy;
     float *h_coords, *h_out, *d_coords, *d_out;
     sg_eval_args *h_args, *d_args;
-    int32_t *h_items, *d_items;
+    int32_t *h_items, *d_items;   /* evaluation CTAs, grouped by dimension */
+    int32_t *h_citems, *d_citems; /* combine CTAs of the split requests     */
+    float *d_part;                /* parts of split sums                    */
     srv_req *reqs[SRV_MAX_REQS];
-    int64_t out_off[SRV_MAX_REQS];
+    int64_t out_off[SRV_MAX_REQS], coord_off[SRV_MAX_REQS], part_off[SRV_MAX_REQS];
+    int order[SRV_MAX_REQS];
     int nreq;
 } srv_slot;
 
@@ -225,13 +245,14 @@ static double now_ms(void)
     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
+/* Delivers a finished batch (lock held; the results were copied into the
+ * callers' buffers beforehand, outside the lock). */
 static void finish_slot(sg_server *s, srv_slot *sl, int ok)
 {
     const double t = now_ms();
     int i;
     for (i = 0; i < sl->nreq; i++) {
         srv_req *r = sl->reqs[i];
-        if (ok) memcpy(r->out, sl->h_out + sl->out_off[i], (size_t)r->m * sizeof(float));
         r->t_done = t;
         r->state = ok ? 2 : 3;
         s->grids[r->gi].pins--;
@@ -242,10 +263,11 @@ static void finish_slot(sg_server *s, srv_slot *sl, int ok)
     pthread_cond_broadcast(&s->cv_done);
 }
 
-/* Fills slot sl with queued requests (lock held) and returns their count. */
+/* Moves queued requests into slot sl (lock held): pointers and offsets
+ * only; returns their count. */
 static int take_batch(sg_server *s, srv_slot *sl)
 {
-    int64_t pts = 0, coff = 0;
+    int64_t pts = 0, coff = 0, poff = 0;
     sl->nreq = 0;
     while (s->head && sl->nreq < SRV_MAX_REQS) {
         srv_req *r = s->head;
@@ -254,10 +276,13 @@ static int take_batch(sg_server *s, srv_slot *sl)
         if (!s->head) s->tail = NULL;
         s->queued_points -= r->m;
         r->state = 1;
+        r->S = s->grids[r->gi].g->L.S;
+        r->g = s->grids[r->gi].g; /* pinned: stays resident until delivered */
         sl->reqs[sl->nreq] = r;
         sl->out_off[sl->nreq] = pts;
-        memcpy(sl->h_coords + coff, r->coords, (size_t)(r->m * r->d) * sizeof(float));
-        sg_grid_eval_args(s->grids[r->gi].g, sl->d_coords + coff, sl->d_out + pts, r->m, &sl->h_args[sl->nreq]);
+        sl->coord_off[sl->nreq] = coff;
+        sl->part_off[sl->nreq] = poff;
+        if (r->g->nparts > 1) poff += r->m * r->g->nparts;
         coff += r->m * r->d;
         pts += r->m;
         sl->nreq++;
@@ -265,43 +290,100 @@ static int take_batch(sg_server *s, srv_slot *sl)
     return sl->nreq;
 }
 
-/* Copies in, one batched evaluation launch per dimension, copies out. */
+/* order[] of a dimension's requests: most subspaces first */
+static void sort_by_subspaces(srv_slot *sl, int lo, int hi)
+{
+    int i, j;
+    for (i = lo + 1; i < hi; i++) {
+        const int v = sl->order[i];
+        const int64_t key = sl->reqs[v]->S;
+        for (j = i; j > lo && sl->reqs[sl->order[j - 1]]->S < key; j--) sl->order[j] = sl->order[j - 1];
+        sl->order[j] = v;
+    }
+}
+
+/* Stages the slot's coordinates and kernel arguments (no lock), copies in,
+ * forks one launch per dimension onto its own stream, joins, copies out. */
 static int launch_batch(sg_server *s, srv_slot *sl)
 {
-    int64_t coff = 0, pts = 0, ni = 0;
-    int i, d, e;
-    int first[SG_MAX_DIMS + 1], count[SG_MAX_DIMS + 1];
+    int64_t coff = 0, pts = 0, ni = 0, nc = 0;
+    int i, d, e, no = 0;
+    int first[SG_MAX_DIMS + 1], count[SG_MAX_DIMS + 1], ppt[SG_MAX_DIMS + 1];
+    (void)s;
     for (i = 0; i < sl->nreq; i++) {
-        coff += sl->reqs[i]->m * sl->reqs[i]->d;
-        pts += sl->reqs[i]->m;
+        srv_req *r = sl->reqs[i];
+        int64_t p;
+        memcpy(sl->h_coords + sl->coord_off[i], r->coords, (size_t)(r->m * r->d) * sizeof(float));
+        sg_grid_eval_args(r->g, sl->d_coords + sl->coord_off[i], sl->d_out + sl->out_off[i], r->m, &sl->h_args[i]);
+        if (sl->h_args[i].nparts > 1) {
+            sl->h_args[i].part_out = sl->d_part + sl->part_off[i];
+            for (p = 0; p < r->m; p += SRV_CTA_THREADS) {
+                sl->h_citems[2 * nc] = i;
+                sl->h_citems[2 * nc + 1] = (int32_t)p;
+                nc++;
+            }
+        }
+        coff += r->m * r->d;
+        pts += r->m;
     }
     for (d = 1; d <= SG_MAX_DIMS; d++) {
+        const int lo = no;
+        int64_t chain = 0, cta;
         first[d] = (int)ni;
-        for (i = 0; i < sl->nreq; i++) {
-            int64_t p;
-            if (sl->reqs[i]->d != d) continue;
-            for (p = 0; p < sl->reqs[i]->m; p += SG_SERVER_CTA_POINTS) {
-                sl->h_items[2 * ni] = i;
-                sl->h_items[2 * ni + 1] = (int32_t)p;
-                ni++;
+        for (i = 0; i < sl->nreq; i++)
+            if (sl->reqs[i]->d == d) {
+                const int64_t c = sl->reqs[i]->S / sl->h_args[i].nparts;
+                sl->order[no++] = i;
+                if (c > chain) chain = c;
             }
+        sort_by_subspaces(sl, lo, no);
+        ppt[d] = chain >= SRV_LONG_CHAIN ? 1 : 2;
+        cta = (int64_t)SRV_CTA_THREADS * ppt[d];
+        for (i = lo; i < no; i++) {
+            const int q = sl->order[i], np = sl->h_args[q].nparts;
+            int64_t p;
+            int k;
+            for (p = 0; p < sl->reqs[q]->m; p += cta)
+                for (k = 0; k < np; k++) {
+                    sl->h_items[2 * ni] = q | (k << 29);
+                    sl->h_items[2 * ni + 1] = (int32_t)p;
+                    ni++;
+                }
         }
         count[d] = (int)ni - first[d];
     }
     if (cudaMemcpyAsync(sl->d_coords, sl->h_coords, (size_t)coff * 4, cudaMemcpyHostToDevice, sl->st) != cudaSuccess ||
         cudaMemcpyAsync(sl->d_args, sl->h_args, (size_t)sl->nreq * sizeof(sg_eval_args), cudaMemcpyHostToDevice,
                         sl->st) != cudaSuccess ||
-        cudaMemcpyAsync(sl->d_items, sl->h_items, (size_t)ni * 8, cudaMemcpyHostToDevice, sl->st) != cudaSuccess)
+        cudaMemcpyAsync(sl->d_items, sl->h_items, (size_t)ni * 8, cudaMemcpyHostToDevice, sl->st) != cudaSuccess ||
+        (nc && cudaMemcpyAsync(sl->d_citems, sl->h_citems, (size_t)nc * 8, cudaMemcpyHostToDevice, sl->st) !=
+                   cudaSuccess) ||
+        cudaEventRecord(sl->ev_in, sl->st) != cudaSuccess)
         return SG_ERR_CUDA;
     for (d = 1; d <= SG_MAX_DIMS; d++) {
         if (!count[d]) continue;
-        e = sgk_evaluate_batch(d, sl->d_args, sl->d_items + 2 * (int64_t)first[d], count[d], 2, sl->st);
-        if (e != cudaSuccess) return SG_ERR_CUDA;
+        if (cudaStreamWaitEvent(sl->dst[d], sl->ev_in, 0) != cudaSuccess) return SG_ERR_CUDA;
+        e = sgk_evaluate_batch(d, sl->d_args, sl->d_items + 2 * (int64_t)first[d], count[d], ppt[d], sl->dst[d]);
+        if (e != cudaSuccess || cudaEventRecord(sl->ev_d[d], sl->dst[d]) != cudaSuccess ||
+            cudaStreamWaitEvent(sl->st, sl->ev_d[d], 0) != cudaSuccess)
+            return SG_ERR_CUDA;
     }
+    if (nc && sgk_combine_parts(sl->d_args, sl->d_citems, (int)nc, sl->st) != cudaSuccess) return SG_ERR_CUDA;
     if (cudaMemcpyAsync(sl->h_out, sl->d_out, (size_t)pts * 4, cudaMemcpyDeviceToHost, sl->st) != cudaSuccess ||
         cudaEventRecord(sl->done, sl->st) != cudaSuccess)
         return SG_ERR_CUDA;
     return SG_OK;
+}
+
+/* Copies a finished slot's results into the callers' buffers (no lock:
+ * the requests are not visible as done until finish_slot). */
+static void deliver(srv_slot *sl)
+{
+    int i;
+    for (i = 0; i < sl->nreq; i++) {
+        srv_req *r = sl->reqs[i];
+        memcpy(r->out, sl->h_out + sl->out_off[i], (size_t)r->m * sizeof(float));
+    }
 }
 
 static void *dispatcher(void *arg)
@@ -313,10 +395,15 @@ static void *dispatcher(void *arg)
         int i, any_busy = 0, free_slot = -1;
         for (i = 0; i < SRV_SLOTS; i++) {
             srv_slot *sl = &s->slot[(s->st_batches + i) % SRV_SLOTS];
-            if (sl->busy) {
+            if (sl->busy == 1) {
                 cudaError_t q = cudaEventQuery(sl->done);
-                if (q == cudaSuccess) finish_slot(s, sl, 1);
-                else if (q != cudaErrorNotReady) {
+                if (q == cudaSuccess) {
+                    sl->busy = 2; /* delivering: not free, not polled */
+                    pthread_mutex_unlock(&s->mu);
+                    deliver(sl);
+                    pthread_mutex_lock(&s->mu);
+                    finish_slot(s, sl, 1);
+                } else if (q != cudaErrorNotReady) {
                     finish_slot(s, sl, 0);
                     s->fatal = 1;
                 }
@@ -358,10 +445,12 @@ static void *dispatcher(void *arg)
     /* drain: wait for running batches, fail what is still queued */
     for (int i = 0; i < SRV_SLOTS; i++)
         if (s->slot[i].busy) {
+            int ok;
             pthread_mutex_unlock(&s->mu);
-            cudaEventSynchronize(s->slot[i].done);
+            ok = cudaEventSynchronize(s->slot[i].done) == cudaSuccess;
+            if (ok) deliver(&s->slot[i]);
             pthread_mutex_lock(&s->mu);
-            finish_slot(s, &s->slot[i], 1);
+            finish_slot(s, &s->slot[i], ok);
         }
     while (s->head) {
         srv_req *r = s->head;
@@ -377,15 +466,23 @@ static void *dispatcher(void *arg)
 
 static void free_slots(sg_server *s)
 {
-    int i;
+    int i, d;
     for (i = 0; i < SRV_SLOTS; i++) {
         srv_slot *sl = &s->slot[i];
         if (sl->st) cudaStreamDestroy(sl->st);
         if (sl->done) cudaEventDestroy(sl->done);
+        if (sl->ev_in) cudaEventDestroy(sl->ev_in);
+        for (d = 0; d <= SG_MAX_DIMS; d++) {
+            if (sl->dst[d]) cudaStreamDestroy(sl->dst[d]);
+            if (sl->ev_d[d]) cudaEventDestroy(sl->ev_d[d]);
+        }
         cudaFreeHost(sl->h_coords);
         cudaFreeHost(sl->h_out);
         cudaFreeHost(sl->h_args);
         cudaFreeHost(sl->h_items);
+        cudaFreeHost(sl->h_citems);
+        cudaFree(sl->d_citems);
+        cudaFree(sl->d_part);
         cudaFree(sl->d_coords);
         cudaFree(sl->d_out);
         cudaFree(sl->d_args);
@@ -409,7 +506,7 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
     }
     s->cap_bytes = hbm_cap_bytes;
     s->max_points = max_batch_points;
-    max_items = (max_batch_points + SG_SERVER_CTA_POINTS - 1) / SG_SERVER_CTA_POINTS + SRV_MAX_REQS;
+    max_items = ((max_batch_points + SRV_CTA_THREADS - 1) / SRV_CTA_THREADS + SRV_MAX_REQS) * SG_EVAL_MAX_PARTS;
     pthread_mutex_init(&s->mu, NULL);
     pthread_mutex_init(&s->plain_mu, NULL);
     pthread_cond_init(&s->cv_work, NULL);
@@ -421,12 +518,20 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
     for (i = 0; i < SRV_SLOTS; i++) {
         srv_slot *sl = &s->slot[i];
         const size_t cb = (size_t)max_batch_points * SG_MAX_DIMS * 4, ob = (size_t)max_batch_points * 4;
-        if (cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+        int ok = 1, d;
+        for (d = 1; d <= SG_MAX_DIMS && ok; d++)
+            ok = cudaStreamCreateWithPriority(&sl->dst[d], cudaStreamNonBlocking, prio_high) == cudaSuccess &&
+                 cudaEventCreateWithFlags(&sl->ev_d[d], cudaEventDisableTiming) == cudaSuccess;
+        if (!ok || cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&sl->ev_in, cudaEventDisableTiming) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_coords, cb) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_out, ob) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_args, SRV_MAX_REQS * sizeof(sg_eval_args)) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_items, (size_t)max_items * 8) != cudaSuccess ||
+            cudaMallocHost((void **)&sl->h_citems, (size_t)max_items * 8) != cudaSuccess ||
+            cudaMalloc((void **)&sl->d_citems, (size_t)max_items * 8) != cudaSuccess ||
+            cudaMalloc((void **)&sl->d_part, ob * SG_EVAL_MAX_PARTS) != cudaSuccess ||
             cudaMalloc((void **)&sl->d_coords, cb) != cudaSuccess || cudaMalloc((void **)&sl->d_out, ob) != cudaSuccess ||
             cudaMalloc((void **)&sl->d_args, SRV_MAX_REQS * sizeof(sg_eval_args)) != cudaSuccess ||
             cudaMalloc((void **)&sl->d_items, (size_t)max_items * 8) != cudaSuccess) {
@@ -534,6 +639,10 @@ static int build_grid(sg_server *s, int d, int n, const int *limits, int fn, con
     if (r == SG_OK) r = sg_sample_function(g, fn, params, num_params, s->admit_st);
     if (r == SG_OK) r = sg_hierarchize_async(g, s->admit_st);
     if (r == SG_OK) r = sg_grid_prepare_eval(g, s->admit_st);
+    if (r == SG_OK && d >= 4 && g->L.S >= SRV_SPLIT_SUBSPACES) {
+        const int64_t np = g->L.S / SRV_PART_SUBSPACES;
+        r = sg_grid_set_parts(g, np > SG_EVAL_MAX_PARTS ? SG_EVAL_MAX_PARTS : (int)np, s->admit_st);
+    }
     if (r == SG_OK) r = sg_sync(g, s->admit_st);
     if (r != SG_OK) {
         if (g) {

@@ -606,16 +606,19 @@ def run_served(args, rank: int, world: int, local_rank: int):
         burst = serve(make_requests(args.requests, 0.0), 0.0)
         launches = kernel_launches() - l0
 
-    # served results equal the plain single-grid call, bit for bit (a sample)
+    # served results equal the plain single-grid call (a sample): bit for bit,
+    # or within 1e-5 * max|u| + 2e-7 where the server split the sums
     from adaptive_sparse_grid_bench_b200 import SgError
-    checked = 0
+    checked = bitwise = 0
     for kind, g, X in make_requests(64, 0.0):
         try:
             out, _ = srv.wait(srv.submit(g, X))
             want = srv.evaluate_now(g, X)
         except SgError:
             continue  # evicted under a small cap
-        if not np.array_equal(out.view(np.uint32), want.view(np.uint32)):
+        bitwise += int(np.array_equal(out.view(np.uint32), want.view(np.uint32)))
+        err = np.abs(out.astype(np.float64) - want)
+        if not np.all(err <= 1e-5 * max(float(np.max(np.abs(want))), 1e-30) + 2e-7):
             raise RuntimeError("served and plain results differ")
         checked += 1
 
@@ -653,7 +656,7 @@ def run_served(args, rank: int, world: int, local_rank: int):
         "best_rate_with_p99_le_2ms": best,
         "plain_per_request": {"evals_per_s": plain_rate, "requests": len(plain),
                               "p50_ms": float(np.percentile(plat, 50)), "p99_ms": float(np.percentile(plat, 99))},
-        "speedup_vs_plain": burst["evals_per_s"] / plain_rate, "checked_vs_plain": checked,
+        "speedup_vs_plain": burst["evals_per_s"] / plain_rate, "checked_vs_plain": checked, "bitwise_vs_plain": bitwise,
         "admit_ms_per_grid_initial": 1e3 * admit_s / ngrid, "server_stats": st,
         "gpu_launches": int(launches), "clocks": clk.summary(),
     }

@@ -11,8 +11,24 @@ from adaptive_sparse_grid_bench_b200 import _lib, inputs
 
 pytestmark = pytest.mark.gpu
 
+# the last two have >= 4096 subspaces: the server splits their sums into
+# parts (3 and 8) evaluated by separate CTAs and added in part order
 SHAPES = [(4, 8, _lib.SG_FN_PROD4, ()), (10, 5, _lib.SG_FN_GAUSS, ()), (2, 9, _lib.SG_FN_BUMP, (0.3, 50.0)),
-          (7, 6, _lib.SG_FN_GAUSS, ()), (12, 4, _lib.SG_FN_PROD4, ())]
+          (7, 6, _lib.SG_FN_GAUSS, ()), (12, 4, _lib.SG_FN_PROD4, ()), (10, 7, _lib.SG_FN_GAUSS, ()),
+          (8, 9, _lib.SG_FN_BUMP, (0.3, 50.0))]
+SPLIT_SUBSPACES = 4096
+# split sums are added in another order than the single-grid kernel's:
+# same tolerance as the parity tests against the FP64 oracle
+RTOL_NORM, ATOL = 1e-5, 2e-7
+
+
+def assert_same_or_close(got, want, split):
+    if not split:
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+        return
+    scale = max(float(np.max(np.abs(want))), 1e-30)
+    err = np.abs(got.astype(np.float64) - want.astype(np.float64))
+    assert np.all(err <= RTOL_NORM * scale + ATOL), f"max err {err.max():.3e}"
 
 
 def _server(cap=8 << 30):
@@ -34,27 +50,52 @@ def test_server_results_equal_single_grid(cuda):
         out, lat = srv.wait(t)
         want = srv.evaluate_now(ids[g], X)
         assert lat >= 0
-        assert np.array_equal(out.view(np.uint32), want.view(np.uint32))
+        d, n = SHAPES[g][:2]
+        assert_same_or_close(out, want, d >= 4 and sg.Grid(d, n).num_subspaces >= SPLIT_SUBSPACES)
     st = srv.stats()
     assert st["requests"] == 40 and st["failed"] == 0 and st["batches"] >= 1
     srv.close()
 
 
-def test_same_result_alone_and_in_mix(cuda):
+@pytest.mark.parametrize("mine_g", [1, 5, 6])
+def test_same_result_alone_and_in_mix(cuda, mine_g):
+    # bit for bit, split grids (5, 6) included: a grid's parts are fixed at
+    # admission, whatever else is in the batch
     srv, ids = _server()
-    X = inputs.uniform_points(7, 20000, SHAPES[1][0])
-    alone, _ = srv.wait(srv.submit(ids[1], X))
+    X = inputs.uniform_points(7, 20000, SHAPES[mine_g][0])
+    X[:3] = [[0.0] * X.shape[1], [1.0] * X.shape[1], [np.nan] * X.shape[1]]  # edges and NaN
+    alone, _ = srv.wait(srv.submit(ids[mine_g], X))
     mix = []
     for q in range(64):
         g = q % len(ids)
         mix.append(srv.submit(ids[g], inputs.uniform_points(100 + q, 1 + 997 * q % 40000, SHAPES[g][0])))
         if q == 31:
-            mine = srv.submit(ids[1], X)
+            mine = srv.submit(ids[mine_g], X)
     for t in mix:
         srv.wait(t)
     in_mix, _ = srv.wait(mine)
     assert np.array_equal(alone.view(np.uint32), in_mix.view(np.uint32))
+    assert alone[1] == 0.0 and np.isnan(alone[2])
     assert srv.stats()["batches"] >= 2
+    srv.close()
+
+
+def test_split_sums_match_oracle(cuda):
+    # the split evaluation against the FP64 oracle directly
+    from oracle.oracle import Oracle
+    srv, ids = _server()
+    for g in (5, 6):
+        d, n = SHAPES[g][:2]
+        grid = sg.Grid(d, n)
+        grid.sample_function(SHAPES[g][2], SHAPES[g][3])
+        vals = grid.get_values()
+        o = Oracle(d, n)
+        s64 = o.hierarchize_f64(vals.astype(np.float64))
+        X = inputs.uniform_points(900 + g, 700, d)
+        out, _ = srv.wait(srv.submit(ids[g], X))
+        ref = o.evaluate_f64(s64, X)
+        scale = max(float(np.max(np.abs(ref))), 1e-30)
+        assert np.max(np.abs(out - ref)) <= RTOL_NORM * scale + ATOL
     srv.close()
 
 
@@ -91,7 +132,9 @@ def test_submissions_from_several_threads(cuda):
                 g = (k + q) % len(ids)
                 X = inputs.uniform_points(1000 * k + q, 1 + (q * 131) % 5000, SHAPES[g][0])
                 out, _ = srv.wait(srv.submit(ids[g], X))
-                if not np.array_equal(out, srv.evaluate_now(ids[g], X)):
+                want = srv.evaluate_now(ids[g], X)
+                scale = max(float(np.max(np.abs(want))), 1e-30)
+                if not np.all(np.abs(out - want) <= RTOL_NORM * scale + ATOL):
                     errors.append((k, q))
         except Exception as exc:  # pragma: no cover - reported below
             errors.append(repr(exc))
