@@ -1,0 +1,6 @@
+/* Evaluation kernels for d = 6 (see eval_impl.cuh); one dimension per file
+ * so the instantiations compile in parallel. */
+#include "eval_impl.cuh"
+
+template int eval_launch<6>(const EvalArgs &, int, void *);
+template int eval_batch_launch<6>(const EvalArgs *, const int2 *, int, int, void *);

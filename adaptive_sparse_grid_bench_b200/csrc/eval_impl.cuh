@@ -27,6 +27,12 @@
  *     its dims has the regular shape whatever the limits, so limit-vector
  *     (adaptive) grids take the unrolled code too; a generic loop covers
  *     budgets above the limits, budgets >= kNB and d = 1;
+ *   - most blocks sit under walk nodes of small remaining budget (at d=10,
+ *     n=10, 8,008 of 11,440 blocks hold at most 4 subspaces), where loop and
+ *     dispatch cost more than the gathers: the last prefix dim with budget
+ *     <= kLG (levels and blocks) and the last two with budget <= 3 run as
+ *     fully unrolled code with compile-time block sizes, in walk order, so
+ *     results are bit-identical to the loop (d <= kMaxUnrollD);
  *   - per prefix dim the walk keeps three values per point: the fractional
  *     part y = frac(x 2^l) (next level: doubling, exact in FP32), the cell
  *     index of the prefix (next level: 2*ix + bit) and the parent's product;
@@ -48,7 +54,7 @@ namespace sgeval {
 
 constexpr int kThreads = 256;
 constexpr int kNB = 10; /* 2-D sub-blocks of budget r < kNB run fully unrolled */
-constexpr int kRF = 3;  /* 3-D blocks of budget R <= kRF run fully unrolled    */
+constexpr int kRF = 5;  /* 3-D blocks of budget R <= kRF run fully unrolled    */
 constexpr int kTB = 15; /* T = floor(x 2^15) holds the cells of levels 0..15   */
 
 __device__ __forceinline__ void kahan_add(float &s, float &c, float v)
@@ -218,6 +224,8 @@ __device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<
             case 0: block3_planes<0, 0, P>(A.alpha, base, in, s); return;
             case 1: block3_planes<1, 0, P>(A.alpha, base, in, s); return;
             case 2: block3_planes<2, 0, P>(A.alpha, base, in, s); return;
+            case 3: block3_planes<3, 0, P>(A.alpha, base, in, s); return;
+            case 4: block3_planes<4, 0, P>(A.alpha, base, in, s); return;
             default: block3_planes<kRF, 0, P>(A.alpha, base, in, s); return;
             }
         }
@@ -257,6 +265,61 @@ struct Range {
     bool partial;
 };
 
+constexpr int kLG = 3;
+/* unrolled subtrees are instantiated for d <= kMaxUnrollD only (their code
+ * grows with d; grids of more dims keep the loop) */
+constexpr int kMaxUnrollD = 12;
+
+/* Levels l = L..B of the last prefix dim and their 3-D blocks of budget
+ * B - l, fully unrolled (every shape regular: B within the limits). */
+template <int D, int P, int B, int L>
+__device__ __forceinline__ void leaf_group(const EvalArgs &A, uint32_t &cur, const Inner<P> &in,
+                                           const float (&pin)[P], float (&y)[P], uint32_t (&ix)[P], float (&acc)[P])
+{
+    if constexpr (L > 0) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) ix[p] = 2 * ix[p] + step_y(y[p]);
+    }
+    constexpr int R = B - L;
+    constexpr uint32_t blk = coff_reg(R, R + 1);
+    uint32_t base[P];
+    float s[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) base[p] = cur + ix[p] * blk;
+    cur += blk << (A.nm1 - R);
+    block3_planes<R, 0, P>(A.alpha, base, in, s);
+#pragma unroll
+    for (int p = 0; p < P; ++p) acc[p] = fmaf(pin[p] * hat_of(y[p]), s[p], acc[p]);
+    if constexpr (L < B) leaf_group<D, P, B, L + 1>(A, cur, in, pin, y, ix, acc);
+}
+
+/* Levels l = L..B of prefix dim K = D-5, each followed by the unrolled
+ * leaf group of dim D-4 with budget B - l (one compensated add per group,
+ * as in the walk). */
+template <int D, int K, int P, int B, int L>
+__device__ __forceinline__ void leaf_group2(const EvalArgs &A, const float *sx, int tid, uint32_t &cur,
+                                            const Inner<P> &in, const float (&pin)[P], float (&y)[P],
+                                            uint32_t (&ix)[P], float (&sum)[P], float (&comp)[P])
+{
+    if constexpr (L > 0) {
+#pragma unroll
+        for (int p = 0; p < P; ++p) ix[p] = 2 * ix[p] + step_y(y[p]);
+    }
+    float pn[P], y2[P], acc[P];
+    uint32_t ix2[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        pn[p] = pin[p] * hat_of(y[p]);
+        y2[p] = sx[((K + 1) * P + p) * kThreads + tid];
+        ix2[p] = ix[p];
+        acc[p] = 0.0f;
+    }
+    leaf_group<D, P, B - L, 0>(A, cur, in, pn, y2, ix2, acc);
+#pragma unroll
+    for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], acc[p]);
+    if constexpr (L < B) leaf_group2<D, K, P, B, L + 1>(A, sx, tid, cur, in, pin, y, ix, sum, comp);
+}
+
 /* Walk over prefix dim K (K <= D-4); children of depth D-4 are blocks.
  * SPLIT: the caller may ask for a block range (batched launches). */
 template <int D, int K, int P, bool SPLIT>
@@ -274,6 +337,33 @@ struct Walk {
             y[p] = sx[(K * P + p) * kThreads + tid];
             ix[p] = ixin[p];
             acc[p] = 0.0f;
+        }
+        if constexpr (D <= kMaxUnrollD && K + 1 == D - 4) {
+            if (!(SPLIT && rg.partial) && budget <= 3 && budget <= A.lim[K] && budget <= A.lim[K + 1] &&
+                budget <= A.lim3) {
+                switch (budget) {
+                case 0: leaf_group2<D, K, P, 0, 0>(A, sx, tid, cur, in, pin, y, ix, sum, comp); break;
+                case 1: leaf_group2<D, K, P, 1, 0>(A, sx, tid, cur, in, pin, y, ix, sum, comp); break;
+                case 2: leaf_group2<D, K, P, 2, 0>(A, sx, tid, cur, in, pin, y, ix, sum, comp); break;
+                case 3: leaf_group2<D, K, P, 3, 0>(A, sx, tid, cur, in, pin, y, ix, sum, comp); break;
+                default: break;
+                }
+                return;
+            }
+        }
+        if constexpr (D <= kMaxUnrollD && K == D - 4) {
+            if (!(SPLIT && rg.partial) && budget <= kLG && budget <= A.lim[K] && budget <= A.lim3) {
+                switch (budget) {
+                case 0: leaf_group<D, P, 0, 0>(A, cur, in, pin, y, ix, acc); break;
+                case 1: leaf_group<D, P, 1, 0>(A, cur, in, pin, y, ix, acc); break;
+                case 2: leaf_group<D, P, 2, 0>(A, cur, in, pin, y, ix, acc); break;
+                case 3: leaf_group<D, P, 3, 0>(A, cur, in, pin, y, ix, acc); break;
+                default: break;
+                }
+#pragma unroll
+                for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], acc[p]);
+                return;
+            }
         }
         for (int l = 0; l <= lmax; ++l) {
             if (l) {
