@@ -28,7 +28,6 @@ SG_HIER_FP64 = 1
 SG_OPT_HIER_PRECISION = 1
 SG_OPT_EVAL_SORT = 2
 SG_OPT_EVAL_PPT = 3
-SG_OPT_EVAL_BLOCKS = 4
 SG_OPT_HIER_KERNEL = 5
 SG_OPT_PROFILE = 6
 SG_OPT_USE_GRAPH = 7
@@ -41,6 +40,7 @@ SG_FN_BUMP = 3
 SG_FN_QUAD = 4
 
 SG_MAX_DIMS = 20
+SG_TUNE_TIMINGS = 6
 SG_MAX_LEVELS = 16
 SG_NOALLOC_MAX_POINTS = 1 << 18
 SG_NOALLOC_SCRATCH_BYTES = 24 << 20
@@ -72,6 +72,7 @@ SIGNATURES = {
     "sg_evaluate_device": (_i, [_p, _p, _p, _i64, _p]),
     "sg_evaluate_device_noalloc": (_i, [_p, _p, _p, _i64, _p]),
     "sg_sync": (_i, [_p, _p]),
+    "sg_autotune": (_i, [_p, _p, _p, _i64, _p, _p]),
     "sg_idx2gp_device": (_i, [_p, _p, _p, _p, _i64, _p]),
     "sg_gp2idx_device": (_i, [_p, _p, _p, _p, _i64, _p]),
     "sg_set_option": (_i, [_p, _i, _i64]),
@@ -98,6 +99,7 @@ SIGNATURES = {
     "sg_batch_sync": (_i, [_p, _p]),
     "sg_batch_set_option": (_i, [_p, _i, _i64]),
     "sg_batch_device_bytes": (_i, [_p, _pi64]),
+    "sg_batch_autotune": (_i, [_p, _p, _p, _p, _p, _p]),
     "sg_server_create": (_i, [_i64, _i64, C.POINTER(_p)]),
     "sg_server_destroy": (_i, [_p]),
     "sg_server_add_grid": (_i, [_p, _i, _i, _p, _i, _p, _i, _pi64]),

@@ -48,7 +48,13 @@ struct sg_batch {
     int64_t *eval_pt_off;
     const float *eval_coords;
     float *eval_out;
-    int eval_ppt;
+    int ppt_d[SG_MAX_DIMS + 1];      /* points per thread per dimension (0: ppt) */
+    int eval_ppt_d[SG_MAX_DIMS + 1]; /* the setting the current plan was built for */
+    int *order;                      /* grids by dimension, most subspaces first */
+    /* the per-dimension launches of an evaluation fork onto their own
+     * streams (joined back before the caller's stream continues) */
+    cudaStream_t dst[SG_MAX_DIMS + 1];
+    cudaEvent_t ev_fork, ev_d[SG_MAX_DIMS + 1];
     cudaGraphExec_t hier_graph, eval_graph;
 };
 

@@ -66,7 +66,6 @@ SG_API int sg_create(int d, int n, const int *limits, sg_grid **grid)
     g->opt[SG_OPT_HIER_PRECISION] = SG_HIER_FP32;
     g->opt[SG_OPT_EVAL_SORT] = 1;
     g->opt[SG_OPT_EVAL_PPT] = 0;
-    g->opt[SG_OPT_EVAL_BLOCKS] = 0;
     g->opt[SG_OPT_HIER_KERNEL] = 0;
     *grid = g;
     return SG_OK;
@@ -508,6 +507,110 @@ SG_API int sg_hierarchize(sg_grid *g)
     return sg_sync(g, 0);
 }
 
+/* Device milliseconds of the fastest of `reps` runs of fn on st. */
+static int time_best(int (*fn)(sg_grid *, void *), sg_grid *g, void *arg, cudaStream_t st, int reps, double *ms)
+{
+    cudaEvent_t e0 = NULL, e1 = NULL;
+    float t;
+    int i, r = SG_OK;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    *ms = 1e30;
+    for (i = 0; e == cudaSuccess && r == SG_OK && i < reps; i++) {
+        e = cudaEventRecord(e0, st);
+        if (e == cudaSuccess) r = fn(g, arg);
+        if (e == cudaSuccess && r == SG_OK) e = cudaEventRecord(e1, st);
+        if (e == cudaSuccess && r == SG_OK) e = cudaEventSynchronize(e1);
+        if (e == cudaSuccess && r == SG_OK) e = cudaEventElapsedTime(&t, e0, e1);
+        if (e == cudaSuccess && r == SG_OK && t < *ms) *ms = t;
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (r == SG_OK && e != cudaSuccess) r = cuda_fail(e, "sg_autotune timing");
+    return r;
+}
+
+typedef struct tune_eval_arg {
+    const float *coords;
+    float *out;
+    int64_t m;
+    cudaStream_t st;
+    const float *saved; /* hierarchization: nodal values to restore first */
+} tune_eval_arg;
+
+static int tune_eval_once(sg_grid *g, void *a)
+{
+    const tune_eval_arg *t = (const tune_eval_arg *)a;
+    return sg_evaluate_device(g, t->coords, t->out, t->m, t->st);
+}
+
+static int tune_hier_once(sg_grid *g, void *a)
+{
+    const tune_eval_arg *t = (const tune_eval_arg *)a;
+    cudaError_t e = cudaMemcpyAsync(g->d_alpha, t->saved, (size_t)g->L.Npad * 4, cudaMemcpyDeviceToDevice, t->st);
+    if (e != cudaSuccess) return cuda_fail(e, "sg_autotune restore");
+    return hierarchize_on(g, t->st);
+}
+
+SG_API int sg_autotune(sg_grid *g, const float *coords, float *out, int64_t num_evals, void *stream, double *ms)
+{
+    static const int ppts[2] = {1, 2};
+    tune_eval_arg ta;
+    double t[SG_TUNE_TIMINGS], best = 1e30;
+    float *saved = NULL;
+    int prev, r = SG_OK, i, j, k, chains_apply = 0, bi = -1;
+    if (!g || !coords || !out || num_evals < 1) return fail(SG_ERR_ARG, "sg_autotune: bad argument");
+    if (!g->has_values) return fail(SG_ERR_STATE, "sg_autotune: no values have been set");
+    if ((r = enter(g, &prev)) != SG_OK) return r;
+    for (i = 0; i < SG_TUNE_TIMINGS; i++) t[i] = -1.0;
+    ta.coords = coords;
+    ta.out = out;
+    ta.m = num_evals;
+    ta.st = (cudaStream_t)stream;
+    /* evaluation: points per thread x spatial ordering (the per-point
+     * arithmetic is the same in every setting, so results do not change) */
+    for (i = 0; i < 2 && r == SG_OK; i++)
+        for (j = 0; j < 2 && r == SG_OK; j++) {
+            g->opt[SG_OPT_EVAL_PPT] = ppts[i];
+            g->opt[SG_OPT_EVAL_SORT] = j;
+            r = tune_eval_once(g, &ta); /* warm: grows the scratch, builds the block layout */
+            if (r == SG_OK) r = time_best(tune_eval_once, g, &ta, ta.st, 2, &t[2 * i + j]);
+            if (r == SG_OK && t[2 * i + j] < best) best = t[2 * i + j], bi = 2 * i + j;
+        }
+    if (r == SG_OK) {
+        g->opt[SG_OPT_EVAL_PPT] = ppts[bi / 2];
+        g->opt[SG_OPT_EVAL_SORT] = bi % 2;
+    }
+    /* hierarchization: shared-memory chains (where they fit) vs gather; the
+     * values are saved first and restored at the end */
+    for (k = 0; k < g->L.d; k++)
+        if (sgk_chain_smem_bytes(g->opt[SG_OPT_HIER_PRECISION] == SG_HIER_FP64 ? g->sweep[k].cap64 : g->sweep[k].cap32,
+                                 g->opt[SG_OPT_HIER_PRECISION] == SG_HIER_FP64 ? 8 : 4) >= 0)
+            chains_apply = 1;
+    if (r == SG_OK) r = dev_alloc(g, (void **)&saved, g->L.Npad * 4, "sg_autotune saved values");
+    if (r == SG_OK) {
+        cudaError_t e = cudaMemcpyAsync(saved, g->d_alpha, (size_t)g->L.Npad * 4, cudaMemcpyDeviceToDevice, ta.st);
+        if (e != cudaSuccess) r = cuda_fail(e, "sg_autotune save");
+        ta.saved = saved;
+        for (k = chains_apply ? 1 : 2; k <= 2 && r == SG_OK; k++) {
+            g->opt[SG_OPT_HIER_KERNEL] = k;
+            r = tune_hier_once(g, &ta);
+            if (r == SG_OK) r = time_best(tune_hier_once, g, &ta, ta.st, 2, &t[3 + k]);
+        }
+        if (r == SG_OK) g->opt[SG_OPT_HIER_KERNEL] = (t[4] >= 0.0 && t[4] <= t[5]) ? 1 : 2;
+        e = cudaMemcpyAsync(g->d_alpha, saved, (size_t)g->L.Npad * 4, cudaMemcpyDeviceToDevice, ta.st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ta.st);
+        if (r == SG_OK && e != cudaSuccess) r = cuda_fail(e, "sg_autotune restore");
+        g->eval_dirty = 1;
+    }
+    if (saved) dev_free(g, saved);
+    if (saved) g->dev_bytes -= g->L.Npad * 4;
+    if (ms)
+        for (i = 0; i < SG_TUNE_TIMINGS; i++) ms[i] = t[i];
+    leave(g, prev);
+    return r == SG_OK ? sg_sync(g, stream) : r;
+}
+
 SG_API int sg_sync(sg_grid *g, void *stream)
 {
     int prev, r = SG_OK, flag = 0;
@@ -764,9 +867,6 @@ SG_API int sg_set_option(sg_grid *g, int option, int64_t value)
         break;
     case SG_OPT_EVAL_PPT:
         if (value < 0 || value > 2) return fail(SG_ERR_ARG, "SG_OPT_EVAL_PPT is 0, 1 or 2");
-        break;
-    case SG_OPT_EVAL_BLOCKS:
-        if (value < 0 || value > 64) return fail(SG_ERR_ARG, "SG_OPT_EVAL_BLOCKS is 0..64");
         break;
     case SG_OPT_HIER_KERNEL:
         if (value < 0 || value > 2) return fail(SG_ERR_ARG, "SG_OPT_HIER_KERNEL is 0, 1 or 2");

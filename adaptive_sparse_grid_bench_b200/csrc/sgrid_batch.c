@@ -123,6 +123,14 @@ static void free_dev(sg_batch *b)
     free(b->h_items);
     b->h_eval_args = NULL;
     b->h_items = NULL;
+    for (k = 0; k <= SG_MAX_DIMS; k++) {
+        if (b->dst[k]) cudaStreamDestroy(b->dst[k]);
+        if (b->ev_d[k]) cudaEventDestroy(b->ev_d[k]);
+        b->dst[k] = NULL;
+        b->ev_d[k] = NULL;
+    }
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    b->ev_fork = NULL;
 }
 
 SG_API int sg_batch_destroy(sg_batch *b)
@@ -134,6 +142,7 @@ SG_API int sg_batch_destroy(sg_batch *b)
     free(b->doff);
     free(b->boff);
     free(b->eval_pt_off);
+    free(b->order);
     free(b);
     return SG_OK;
 }
@@ -594,12 +603,23 @@ SG_API int sg_batch_hierarchize(sg_batch *b)
 /* Evaluation plan: per-grid kernel arguments and per-dimension CTA items for
  * the caller's point offsets and buffers (kept, so an identical call replays
  * the captured graph). */
+static int ppt_of(const sg_batch *b, int d) { return b->ppt_d[d] ? b->ppt_d[d] : b->ppt; }
+
+static int cmp_dim_then_subspaces(const void *x, const void *y, void *ctx)
+{
+    const sg_batch *b = (const sg_batch *)ctx;
+    const sg_layout *a = &b->L[*(const int *)x], *c = &b->L[*(const int *)y];
+    if (a->d != c->d) return a->d < c->d ? -1 : 1;
+    if (a->S != c->S) return a->S > c->S ? -1 : 1;
+    return *(const int *)x - *(const int *)y;
+}
+
 static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, float *out)
 {
-    int g, k, r;
+    int g, k, r, q;
     int64_t coff = 0, ni = 0, cap_items = 0;
-    const int cta = 256 * b->ppt;
-    int same = b->h_eval_args && b->eval_coords == coords && b->eval_out == out && b->eval_ppt == b->ppt;
+    int same = b->h_eval_args && b->eval_coords == coords && b->eval_out == out;
+    for (k = 0; same && k <= SG_MAX_DIMS; k++) same = b->eval_ppt_d[k] == ppt_of(b, k);
     for (g = 0; same && g <= b->ng; g++) same = b->eval_pt_off[g] == pt_off[g];
     if (same) return SG_OK;
     if (b->eval_graph) {
@@ -617,7 +637,13 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
     for (g = 0; g < b->ng; g++) {
         const int64_t m = pt_off[g + 1] - pt_off[g];
         if (m < 0) return bfail(SG_ERR_ARG, "sg_batch_evaluate: point offsets decrease at grid %d", g);
-        cap_items += (m + cta - 1) / cta;
+        cap_items += (m + 255) / 256; /* enough for one point per thread */
+    }
+    if (!b->order) {
+        b->order = (int *)malloc(sizeof(int) * (size_t)b->ng);
+        if (!b->order) return bfail(SG_ERR_NOMEM, "out of host memory");
+        for (g = 0; g < b->ng; g++) b->order[g] = g;
+        qsort_r(b->order, (size_t)b->ng, sizeof(int), cmp_dim_then_subspaces, b);
     }
     free(b->h_items);
     b->h_items = (int32_t *)malloc((size_t)(cap_items > 0 ? cap_items : 1) * 2 * sizeof(int32_t));
@@ -642,15 +668,18 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
                 p.blk3[s] = p.blk2[s] = 0;
             }
         }
-        p.ppt = b->ppt;
+        p.ppt = ppt_of(b, L->d);
         sgk_fill_eval_args(&p, coords + coff, NULL, out + pt_off[g], pt_off[g + 1] - pt_off[g], &b->h_eval_args[g]);
         coff += (pt_off[g + 1] - pt_off[g]) * L->d;
     }
-    /* items grouped by dimension */
+    /* items grouped by dimension, grids with the most subspaces first (their
+     * CTAs are the longest) */
     for (k = 1; k <= SG_MAX_DIMS; k++) {
+        const int cta = 256 * ppt_of(b, k);
         b->items_first[k] = (int)ni;
-        for (g = 0; g < b->ng; g++) {
+        for (q = 0; q < b->ng; q++) {
             int64_t st;
+            g = b->order[q];
             if (b->L[g].d != k) continue;
             for (st = pt_off[g]; st < pt_off[g + 1]; st += cta) {
                 b->h_items[2 * ni] = g;
@@ -672,20 +701,38 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
     for (g = 0; g <= b->ng; g++) b->eval_pt_off[g] = pt_off[g];
     b->eval_coords = coords;
     b->eval_out = out;
-    b->eval_ppt = b->ppt;
+    for (k = 0; k <= SG_MAX_DIMS; k++) b->eval_ppt_d[k] = ppt_of(b, k);
     return SG_OK;
 }
 
+static int make_fork_streams(sg_batch *b)
+{
+    int k;
+    if (b->ev_fork) return SG_OK;
+    BCU(cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
+    for (k = 1; k <= SG_MAX_DIMS; k++) {
+        BCU(cudaStreamCreateWithFlags(&b->dst[k], cudaStreamNonBlocking), "cudaStreamCreate");
+        BCU(cudaEventCreateWithFlags(&b->ev_d[k], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    return SG_OK;
+}
+
+/* Repack, then one launch per dimension, each on its own stream forked from
+ * and joined back to st (captured as parallel branches of the graph). */
 static int eval_launches(sg_batch *b, cudaStream_t st)
 {
     int k, e;
     if ((e = sgk_repack(b->d_alpha, b->d_blk, b->d_repack, b->nrepack, st)) != cudaSuccess)
         return bcuda((cudaError_t)e, "batch repack");
+    BCU(cudaEventRecord(b->ev_fork, st), "cudaEventRecord");
     for (k = 1; k <= SG_MAX_DIMS; k++) {
         if (!b->items_count[k]) continue;
-        e = sgk_evaluate_batch(k, b->d_eval_args, b->d_items + 2 * (int64_t)b->items_first[k], b->items_count[k], b->ppt,
-                               st);
+        BCU(cudaStreamWaitEvent(b->dst[k], b->ev_fork, 0), "cudaStreamWaitEvent");
+        e = sgk_evaluate_batch(k, b->d_eval_args, b->d_items + 2 * (int64_t)b->items_first[k], b->items_count[k],
+                               ppt_of(b, k), b->dst[k]);
         if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch evaluate");
+        BCU(cudaEventRecord(b->ev_d[k], b->dst[k]), "cudaEventRecord");
+        BCU(cudaStreamWaitEvent(st, b->ev_d[k], 0), "cudaStreamWaitEvent");
     }
     return SG_OK;
 }
@@ -700,9 +747,64 @@ SG_API int sg_batch_evaluate_device(sg_batch *b, const int64_t *point_offsets, c
     if (point_offsets[b->ng] > 0 && (!coords || !out)) return bfail(SG_ERR_ARG, "sg_batch_evaluate_device: NULL buffer");
     if (point_offsets[b->ng] >= ((int64_t)1 << 31)) return bfail(SG_ERR_RANGE, "sg_batch_evaluate: too many points");
     if ((r = enter(b, &prev)) != SG_OK) return r;
-    if ((r = plan_eval(b, point_offsets, coords, out)) == SG_OK)
+    if ((r = make_fork_streams(b)) == SG_OK && (r = plan_eval(b, point_offsets, coords, out)) == SG_OK)
         r = b->use_graph ? run_graph(&b->eval_graph, eval_launches, b, st) : eval_launches(b, st);
     if (r == SG_OK) b->eval_dirty = 0;
+    leave(b, prev);
+    return r;
+}
+
+SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const float *coords, float *out, void *stream,
+                             double *ms)
+{
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0 = NULL, e1 = NULL;
+    double t[2][SG_MAX_DIMS + 1];
+    int prev, r, pi, k, rep;
+    float el;
+    if (!b || !point_offsets || point_offsets[0] != 0) return bfail(SG_ERR_ARG, "sg_batch_autotune: bad argument");
+    if (!b->has_values || b->dev < 0) return bfail(SG_ERR_STATE, "sg_batch_autotune: no values have been set");
+    if (point_offsets[b->ng] > 0 && (!coords || !out)) return bfail(SG_ERR_ARG, "sg_batch_autotune: NULL buffer");
+    if ((r = enter(b, &prev)) != SG_OK) return r;
+    for (pi = 0; pi < 2; pi++)
+        for (k = 0; k <= SG_MAX_DIMS; k++) t[pi][k] = -1.0;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        r = bfail(SG_ERR_CUDA, "sg_batch_autotune: cudaEventCreate");
+        goto done;
+    }
+    if ((r = make_fork_streams(b)) != SG_OK) goto done;
+    /* every dimension's launch alone on st, at 1 and at 2 points per thread */
+    for (pi = 0; pi < 2 && r == SG_OK; pi++) {
+        for (k = 0; k <= SG_MAX_DIMS; k++) b->ppt_d[k] = pi + 1;
+        if ((r = plan_eval(b, point_offsets, coords, out)) != SG_OK) break;
+        if (sgk_repack(b->d_alpha, b->d_blk, b->d_repack, b->nrepack, st) != cudaSuccess) {
+            r = bfail(SG_ERR_CUDA, "sg_batch_autotune: repack");
+            break;
+        }
+        for (k = 1; k <= SG_MAX_DIMS && r == SG_OK; k++) {
+            if (!b->items_count[k]) continue;
+            for (rep = 0; rep < 3; rep++) { /* first run warms */
+                if (cudaEventRecord(e0, st) != cudaSuccess ||
+                    sgk_evaluate_batch(k, b->d_eval_args, b->d_items + 2 * (int64_t)b->items_first[k],
+                                       b->items_count[k], pi + 1, st) != cudaSuccess ||
+                    cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                    cudaEventElapsedTime(&el, e0, e1) != cudaSuccess) {
+                    r = bfail(SG_ERR_CUDA, "sg_batch_autotune: timing d=%d", k);
+                    break;
+                }
+                if (rep > 0 && (t[pi][k] < 0.0 || el < t[pi][k])) t[pi][k] = el;
+            }
+        }
+    }
+    for (k = 0; k <= SG_MAX_DIMS; k++)
+        b->ppt_d[k] = (r == SG_OK && t[0][k] >= 0.0) ? (t[0][k] <= t[1][k] ? 1 : 2) : 0;
+    b->eval_dirty = 1;
+    if (ms)
+        for (pi = 0; pi < 2; pi++)
+            for (k = 0; k <= SG_MAX_DIMS; k++) ms[pi * (SG_MAX_DIMS + 1) + k] = t[pi][k];
+done:
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
     leave(b, prev);
     return r;
 }
@@ -722,6 +824,7 @@ SG_API int sg_batch_set_option(sg_batch *b, int option, int64_t value)
     case SG_OPT_EVAL_PPT:
         if (value < 0 || value > 2) return bfail(SG_ERR_ARG, "SG_OPT_EVAL_PPT is 0, 1 or 2");
         b->ppt = value == 0 ? 2 : (int)value;
+        memset(b->ppt_d, 0, sizeof(b->ppt_d)); /* an explicit setting replaces tuned ones */
         return SG_OK;
     case SG_OPT_USE_GRAPH:
         if (value != 0 && value != 1) return bfail(SG_ERR_ARG, "SG_OPT_USE_GRAPH is 0 or 1");

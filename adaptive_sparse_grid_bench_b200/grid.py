@@ -226,6 +226,17 @@ class Grid:
     def sync(self, stream=None) -> None:
         check(L.lib().sg_sync(self._h, _stream_handle(stream)))
 
+    def autotune(self, coords, out, num_evals: int | None = None, stream=None) -> dict:
+        """sg_autotune: times the evaluation settings and sweep kernels on these
+        device buffers, keeps the fastest; returns the timings (ms, -1 = n/a)."""
+        if num_evals is None:
+            num_evals = int(coords.shape[0])
+        ms = np.zeros(L.SG_TUNE_TIMINGS, np.float64)
+        check(L.lib().sg_autotune(self._h, self._dptr(coords), self._dptr(out), int(num_evals),
+                                  _stream_handle(stream), _ptr(ms)))
+        return {"eval_ppt1_unsorted": ms[0], "eval_ppt1_sorted": ms[1], "eval_ppt2_unsorted": ms[2],
+                "eval_ppt2_sorted": ms[3], "hier_chains": ms[4], "hier_gather": ms[5]}
+
     def idx2gp_device(self, index, levels, indices, count: int, stream=None) -> None:
         check(L.lib().sg_idx2gp_device(self._h, self._dptr(index), self._dptr(levels), self._dptr(indices),
                                        int(count), _stream_handle(stream)))

@@ -61,7 +61,6 @@ extern "C" {
 #define SG_OPT_EVAL_SORT 2      /* 1 (default): spatially order points on the GPU   */
                                 /* before evaluating; 0: evaluate in caller order    */
 #define SG_OPT_EVAL_PPT 3       /* points per thread in evaluate: 0 = auto, 1, 2     */
-#define SG_OPT_EVAL_BLOCKS 4    /* subspace blocking: number of passes, 0 = auto     */
 #define SG_OPT_HIER_KERNEL 5    /* 0 = auto, 1 = shared-memory chains, 2 = gather    */
 #define SG_OPT_PROFILE 6        /* 1: record CUDA events around each phase            */
 #define SG_OPT_USE_GRAPH 7      /* batches: 1 (default) capture launches in a CUDA graph */
@@ -137,6 +136,20 @@ int sg_evaluate_device_noalloc(sg_grid *grid, const float *coord_mat, float *out
 
 /* Waits for `stream` and reports any device-side error flag of the handle. */
 int sg_sync(sg_grid *grid, void *stream);
+
+/* Autotuner (no reference counterpart; the reference tunes its CUDA block
+ * size by hand, run.sh).  Times, on the caller's device buffers and stream,
+ * the evaluation under every setting of points per thread {1, 2} x spatial
+ * ordering {off, on}, and the hierarchization with the shared-memory chain
+ * sweeps (where they fit) and the gather sweeps; keeps the fastest in the
+ * handle's options (SG_OPT_EVAL_PPT, SG_OPT_EVAL_SORT, SG_OPT_HIER_KERNEL).
+ * No setting changes any result.  The grid's values are the same on return
+ * (saved and restored); out[] holds the evaluation.  ms (optional,
+ * SG_TUNE_TIMINGS entries): evaluation ms for (ppt, sort) = (1,0), (1,1),
+ * (2,0), (2,1), then hierarchization ms for chains and gather (-1: not
+ * applicable). */
+#define SG_TUNE_TIMINGS 6
+int sg_autotune(sg_grid *grid, const float *coord_mat, float *out, int64_t num_evals, void *stream, double *ms);
 
 /* Device bijection for batches (no reference counterpart beyond looping
  * gp2idx/idx2gp; used to sample grids on the GPU).  levels/indices are
@@ -218,6 +231,13 @@ int sg_batch_evaluate_device(sg_batch *batch, const int64_t *point_offsets, cons
 int sg_batch_sync(sg_batch *batch, void *stream);
 /* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH */
 int sg_batch_set_option(sg_batch *batch, int option, int64_t value);
+/* Autotuner for the batched evaluation (no reference counterpart): times
+ * each dimension's launch over the caller's points at 1 and at 2 points per
+ * thread and keeps the faster per dimension (results do not change).  Until
+ * the next SG_OPT_EVAL_PPT setting, which replaces it.  ms (optional,
+ * 2*(SG_MAX_DIMS+1) entries): [ppt-1][d] launch ms, -1 where no grid has d. */
+int sg_batch_autotune(sg_batch *batch, const int64_t *point_offsets, const float *coord_mat, float *out,
+                      void *stream, double *ms);
 int sg_batch_device_bytes(const sg_batch *batch, int64_t *bytes);
 
 /* ---- serving loop --------------------------------------------------------

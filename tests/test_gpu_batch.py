@@ -94,3 +94,33 @@ def test_batch_sample_quad_and_config_like_workload(cuda):
         want = one.evaluate(Xs[g])
         assert np.array_equal(res[po[g]:po[g + 1]].view(np.uint32), want.view(np.uint32))
         assert vals.size == b.grid_values(surplus, g).size
+
+
+def test_batch_autotune_keeps_results(cuda):
+    # the autotuner picks points per thread per dimension; results are the
+    # same bits before and after, graph replay included
+    import torch
+    b = _batch(MIXED)
+    vals = inputs.uniform01(79, b.num_values) * 2 - 1
+    b.set_values(vals)
+    b.hierarchize()
+    counts = [5, 1, 513, 1000, 257, 33, 2048, 600, 70, 511, 512, 1025]
+    po = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = torch.from_numpy(np.concatenate(
+        [inputs.uniform_points(300 + g, counts[g], MIXED[g][0]).reshape(-1) for g in range(len(MIXED))])).to(cuda)
+    out = torch.empty(int(po[-1]), device=cuda)
+    b.evaluate_device(po, coords, out)
+    b.sync()
+    before = out.cpu().numpy().copy()
+    ms = b.autotune(po, coords, out)
+    dims_present = sorted({d for d, _, _ in MIXED})
+    for d in range(1, _lib.SG_MAX_DIMS + 1):
+        if d in dims_present:
+            assert ms[0, d] > 0 and ms[1, d] > 0
+        else:
+            assert ms[0, d] == -1 and ms[1, d] == -1
+    out.fill_(float("nan"))
+    for rep in range(2):
+        b.evaluate_device(po, coords, out)
+        b.sync()
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), before.view(np.uint32))

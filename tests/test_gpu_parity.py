@@ -219,3 +219,37 @@ def test_errors_on_gpu(cuda):
     g.set_values(np.ones(g.num_points, np.float32))
     with pytest.raises(ValueError):
         g.set_values(np.ones(g.num_points + 1, np.float32))
+
+
+@pytest.mark.parametrize("d,n,lim,precision", [(4, 8, None, "fp32"), (10, 6, None, "fp64"), (3, 16, None, "fp32"),
+                                               (6, 9, [8, 2, 5, 8, 8, 1], "fp32")])
+def test_autotune_keeps_values_and_results(cuda, d, n, lim, precision):
+    # every setting the autotuner tries gives the same bits; the grid's
+    # values are restored; the chosen options are valid settings
+    import torch
+    g = _grid(d, n, lim)
+    g.precision = precision
+    g.set_values(inputs.uniform01(5, g.num_points) * 2 - 1)
+    g.hierarchize()
+    surplus = g.get_values()
+    X = inputs.uniform_points(6, 5000, d)
+    want = g.evaluate(X)
+    Xd = torch.from_numpy(X).to(cuda)
+    out = torch.empty(X.shape[0], device=cuda)
+    ms = g.autotune(Xd, out)
+    assert all(v > 0 for k, v in ms.items() if k.startswith("eval"))
+    assert ms["hier_gather"] > 0
+    assert np.array_equal(g.get_values().view(np.uint32), surplus.view(np.uint32))
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), want.view(np.uint32))
+    assert g.get_option(sg.SG_OPT_EVAL_PPT) in (1, 2) and g.get_option(sg.SG_OPT_EVAL_SORT) in (0, 1)
+    assert g.get_option(sg.SG_OPT_HIER_KERNEL) in (1, 2)
+    assert np.array_equal(g.evaluate(X).view(np.uint32), want.view(np.uint32))
+    # the tuned sweep kernel still gives hierarchize0's bits
+    g.set_values(inputs.uniform01(7, g.num_points) * 2 - 1)
+    nodal = g.get_values()
+    g.hierarchize()
+    one = _grid(d, n, lim)
+    one.precision = precision
+    one.set_values(nodal)
+    one.hierarchize()
+    assert np.array_equal(g.get_values().view(np.uint32), one.get_values().view(np.uint32))
