@@ -43,15 +43,18 @@ __global__ void __launch_bounds__(kThreads) k_combine_parts(const sg_eval_args *
     A->out[i] = __fsub_rn(s, c);
 }
 
-/* compact (group-aligned) layout -> block layout, one CTA per subspace */
+/* compact (group-aligned) layout -> block layout */
 __global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
                          const sg_repack *__restrict__ rp, int64_t nsub)
 {
-    for (int64_t q = blockIdx.x; q < nsub; q += gridDim.x) {
+    /* one warp per subspace: most subspaces hold a few values, and a warp
+     * per subspace keeps many descriptor loads in flight */
+    const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
+    for (int64_t q = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); q < nsub; q += nw) {
         const sg_repack r = rp[q];
         const int n = 1 << r.s;
         const int ab = r.a + r.b, cab = r.c + ab;
-        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        for (int e = threadIdx.x & 31; e < n; e += 32) {
             const uint32_t I = (uint32_t)e >> cab;
             const uint32_t tc = ((uint32_t)e >> ab) & ((1u << r.c) - 1u);
             const uint32_t ta = ((uint32_t)e >> r.b) & ((1u << r.a) - 1u);
@@ -259,8 +262,9 @@ int sgk_combine_parts(const sg_eval_args *grids, const int32_t *items, int nitem
 int sgk_repack(const float *src, float *dst, const sg_repack *rp, int64_t nsub, void *stream)
 {
     if (nsub <= 0) return cudaSuccess;
-    int64_t g = nsub < 148 * 64 ? nsub : 148 * 64;
-    k_repack<<<(unsigned)g, 128, 0, (cudaStream_t)stream>>>(src, dst, rp, nsub);
+    int64_t g = (nsub + 7) / 8;
+    if (g > 148 * 16) g = 148 * 16;
+    k_repack<<<(unsigned)g, 256, 0, (cudaStream_t)stream>>>(src, dst, rp, nsub);
     sgk_count(1);
     return cudaGetLastError();
 }

@@ -425,6 +425,63 @@ int launch_chains(T *a, const sg_sweep_tables *t, int *err, void *stream)
     return launch_chains_nt<T, 512>(a, t, cap, err, stream);
 }
 
+/* Small chains (the many short chains of batched grids): one warp per
+ * chain.  The warp loads the chain's segments into its own shared-memory
+ * buffer with plain coalesced loads (no bulk copies, barriers or CTA-wide
+ * synchronisation, whose fixed cost dominates a chain of a few hundred
+ * values), then writes each updated point straight to global memory: the
+ * updates read only the pre-sweep values in the buffer, with the same
+ * arithmetic as k_sweep_chains, so results are bit-identical. */
+template <typename T>
+__global__ void __launch_bounds__(256) k_sweep_small(T *__restrict__ a, const sg_chain *__restrict__ chains,
+                                                     const uint32_t *__restrict__ seg, int nch, int cap)
+{
+    constexpr int A = 16 / sizeof(T);
+    extern __shared__ __align__(16) unsigned char smem_small[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    T *buf = reinterpret_cast<T *>(smem_small) + (size_t)w * cap;
+    const int nw = gridDim.x * (blockDim.x >> 5);
+    /* the chain index is the same for all lanes: every loop below is
+     * warp-uniform */
+    for (int c = blockIdx.x * (blockDim.x >> 5) + w; c < nch; c += nw) {
+        const sg_chain ch = chains[c];
+        for (int j = 0; j <= ch.lmax; ++j) {
+            const int n = 1 << (ch.sigma + j);
+            const T *src = a + seg[ch.seg + j];
+            T *dst = buf + seg_soff<A>(ch.sigma, j);
+            for (int p = lane; p < n; p += 32) dst[p] = src[p];
+        }
+        __syncwarp();
+        for (int j = 1; j <= ch.lmax; ++j) {
+            const int n = 1 << (ch.sigma + j);
+            T *out = a + seg[ch.seg + j];
+            for (int p = lane; p < n; p += 32) out[p] = chain_point<T, A>(buf, ch.sigma, ch.lo, j, p);
+        }
+        __syncwarp();
+    }
+}
+
+template <typename T>
+int launch_small(T *a, const sg_sweep_tables *t, void *stream)
+{
+    if (t->nchains == 0) return cudaSuccess;
+    const int64_t cap = sizeof(T) == 4 ? t->cap32 : t->cap64;
+    const int64_t smem = 8 * cap * (int64_t)sizeof(T); /* 8 warps per CTA */
+    if (smem > 200 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_sweep_small<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_small<T>, 256, (size_t)smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (t->nchains + 7) / 8;
+    if (grid > (int64_t)sgk_num_sms() * per_sm) grid = (int64_t)sgk_num_sms() * per_sm;
+    k_sweep_small<T><<<(unsigned)grid, 256, (size_t)smem, (cudaStream_t)stream>>>(a, t->chains, t->seg,
+                                                                                (int)t->nchains, (int)cap);
+    sgk_count(1);
+    return cudaGetLastError();
+}
+
 template <typename T>
 int launch_gather(T *a, const sg_sweep_tables *t, void *stream)
 {
@@ -473,6 +530,19 @@ int sgk_sweep_chains_f32(float *a, const sg_sweep_tables *t, int *err, void *str
 int sgk_sweep_chains_f64(double *a, const sg_sweep_tables *t, int *err, void *stream)
 {
     return launch_chains<double>(a, t, err, stream);
+}
+int sgk_sweep_small_f32(float *a, const sg_sweep_tables *t, void *stream)
+{
+    return launch_small<float>(a, t, stream);
+}
+int sgk_sweep_small_f64(double *a, const sg_sweep_tables *t, void *stream)
+{
+    return launch_small<double>(a, t, stream);
+}
+int64_t sgk_small_smem_bytes(int64_t cap_elems, int elem_bytes)
+{
+    const int64_t b = 8 * cap_elems * elem_bytes;
+    return b <= 200 * 1024 ? b : -1;
 }
 int sgk_sweep_gather_f32(float *a, const sg_sweep_tables *t, void *stream)
 {

@@ -10,6 +10,7 @@
 #include "sg_layout.h"
 
 #define SG_BATCH_CLASSES 4 /* size classes of the shared-memory hierarchization */
+#define SG_SWEEP_CLASSES 3 /* chain size classes of the batched sweeps          */
 
 struct sg_batch {
     int ng;
@@ -19,6 +20,7 @@ struct sg_batch {
     int64_t *boff;       /* offsets in the block-layout buffer, ng+1               */
     int dev, has_values, eval_dirty;
     int precision, ppt, use_graph;
+    int hier_kernel[SG_SWEEP_CLASSES]; /* per chain size class: 0/1 chains (where they fit), 2 gather */
     int64_t dev_bytes;
     float *d_alpha;      /* all grids, group-aligned layout                       */
     double *d_work;      /* FP64 sweep values (lazy)                              */
@@ -35,7 +37,9 @@ struct sg_batch {
     uint32_t *d_smem_seg;
     /* chain-sweep path */
     int has_sweep_grids;
-    sg_sweep_tables sweepB[SG_MAX_DIMS];
+    /* chains of sweep k sorted by size, in SG_SWEEP_CLASSES classes that
+     * launch with their own CTA size and shared-memory stages */
+    sg_sweep_tables sweepB[SG_MAX_DIMS][SG_SWEEP_CLASSES];
     sg_chain *d_chB[SG_MAX_DIMS];
     uint32_t *d_segB[SG_MAX_DIMS];
     /* evaluation */

@@ -35,10 +35,18 @@ int sgk_sweep_chains_f64(double *a, const sg_sweep_tables *t, int *err, void *st
  * parents from global memory (any chain size). */
 int sgk_sweep_gather_f32(float *a, const sg_sweep_tables *t, void *stream);
 int sgk_sweep_gather_f64(double *a, const sg_sweep_tables *t, void *stream);
+/* The same sweep for short chains: one warp per chain, plain loads into a
+ * per-warp shared-memory buffer of cap elements (8 warps per CTA).
+ * sgk_small_smem_bytes < 0: the chains are too long for it. */
+int sgk_sweep_small_f32(float *a, const sg_sweep_tables *t, void *stream);
+int sgk_sweep_small_f64(double *a, const sg_sweep_tables *t, void *stream);
+int64_t sgk_small_smem_bytes(int64_t cap_elems, int elem_bytes);
 int sgk_widen(const float *src, double *dst, int64_t n, void *stream);
 
 /* A run of values at `compact` in a caller's compact array and at `dev` in
- * a device layout. */
+ * a device layout.  Runs are cut into pieces of at most SG_COPY_PIECE
+ * values (one CTA copies one piece at a time). */
+#define SG_COPY_PIECE 8192
 typedef struct sg_copy_seg {
     int64_t compact, dev, count;
 } sg_copy_seg;

@@ -183,6 +183,28 @@ static int upload(sg_batch *b, void **dst, const void *src, int64_t bytes, const
     return SG_OK;
 }
 
+static int make_fork_streams(sg_batch *b);
+
+/* shared-memory elements one chain needs (segments padded to 16 bytes) */
+static int64_t chain_elems(const sg_chain *c, int elem_bytes)
+{
+    const int64_t minsz = 16 / elem_bytes;
+    int64_t e = 0;
+    int j;
+    for (j = 0; j <= c->lmax; j++) {
+        const int64_t sz = (int64_t)1 << (c->sigma + j);
+        e += sz < minsz ? minsz : sz;
+    }
+    return e;
+}
+
+static int cmp_chain_desc(const void *x, const void *y)
+{
+    const int64_t a = chain_elems((const sg_chain *)x, 4), c = chain_elems((const sg_chain *)y, 4);
+    if (a != c) return a > c ? -1 : 1;
+    return ((const sg_chain *)x)->seg < ((const sg_chain *)y)->seg ? -1 : 1;
+}
+
 /* grids that take the shared-memory path, and their size class */
 static int smem_class(const sg_layout *L)
 {
@@ -229,11 +251,12 @@ static int materialize(sg_batch *b)
     if ((r = balloc(b, (void **)&b->d_err, 16, "error flag")) != SG_OK) goto done;
     BCU(cudaMemset(b->d_err, 0, 16), "cudaMemset");
 
-    /* level-group runs for moving values in one launch */
+    /* level-group runs for moving values in one launch, cut into pieces of
+     * at most SG_COPY_PIECE values so that one CTA's share stays bounded */
     {
         int64_t ns = 0;
         sg_copy_seg *segs;
-        for (g = 0; g < b->ng; g++) ns += b->L[g].n;
+        for (g = 0; g < b->ng; g++) ns += b->L[g].n + b->L[g].N / SG_COPY_PIECE;
         segs = (sg_copy_seg *)malloc((size_t)ns * sizeof(sg_copy_seg));
         if (!segs) { r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
         ns = 0;
@@ -241,11 +264,14 @@ static int materialize(sg_batch *b)
             int s;
             const sg_layout *L = &b->L[g];
             for (s = 0; s < L->n; s++) {
-                if (L->lidx[s + 1] == L->lidx[s]) continue;
-                segs[ns].compact = b->voff[g] + L->lidx[s];
-                segs[ns].dev = b->doff[g] + L->plidx[s];
-                segs[ns].count = L->lidx[s + 1] - L->lidx[s];
-                ns++;
+                int64_t at;
+                for (at = L->lidx[s]; at < L->lidx[s + 1]; at += SG_COPY_PIECE) {
+                    const int64_t left = L->lidx[s + 1] - at;
+                    segs[ns].compact = b->voff[g] + at;
+                    segs[ns].dev = b->doff[g] + L->plidx[s] + (at - L->lidx[s]);
+                    segs[ns].count = left < SG_COPY_PIECE ? left : SG_COPY_PIECE;
+                    ns++;
+                }
             }
         }
         b->nsegs = ns;
@@ -328,18 +354,8 @@ static int materialize(sg_batch *b)
             }
             if (!chB[k] || !segB[k]) { free(ch); free(sgo); r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
             for (i = 0; i < nch; i++) {
-                int j;
-                int64_t e32 = 0, e64 = 0;
                 chB[k][nchB[k] + i] = ch[i];
                 chB[k][nchB[k] + i].seg = (uint32_t)(ch[i].seg + nsegB[k]);
-                for (j = 0; j <= ch[i].lmax; j++) {
-                    int64_t sz = (int64_t)1 << (ch[i].sigma + j);
-                    e32 += sz < 4 ? 4 : sz;
-                    e64 += sz < 2 ? 2 : sz;
-                }
-                if (e32 > b->sweepB[k].cap32) b->sweepB[k].cap32 = e32;
-                if (e64 > b->sweepB[k].cap64) b->sweepB[k].cap64 = e64;
-                if (ch[i].lmax > b->sweepB[k].lmax_max) b->sweepB[k].lmax_max = ch[i].lmax;
             }
             for (i = 0; i < nseg; i++) segB[k][nsegB[k] + i] = (uint32_t)(sgo[i] + b->doff[g]);
             nchB[k] += nch;
@@ -349,12 +365,35 @@ static int materialize(sg_batch *b)
         }
     }
     for (k = 0; k < SG_MAX_DIMS; k++) {
+        int64_t i, first[SG_SWEEP_CLASSES + 1];
+        int cls;
+        /* largest chains first, then split by the CTA size they need */
+        if (nchB[k] > 1) qsort(chB[k], (size_t)nchB[k], sizeof(sg_chain), cmp_chain_desc);
+        /* classes are contiguous (sorted by size): count, then prefix sums */
+        for (cls = 0; cls <= SG_SWEEP_CLASSES; cls++) first[cls] = 0;
+        for (i = 0; i < nchB[k]; i++) {
+            const int64_t e32 = chain_elems(&chB[k][i], 4);
+            first[1 + (e32 > 256 * 12 ? 0 : (e32 > 128 * 12 ? 1 : 2))]++;
+        }
+        for (cls = 1; cls <= SG_SWEEP_CLASSES; cls++) first[cls] += first[cls - 1];
         if ((r = upload(b, (void **)&b->d_chB[k], chB[k], nchB[k] * (int64_t)sizeof(sg_chain), "sweep chains")) != SG_OK)
             goto done;
         if ((r = upload(b, (void **)&b->d_segB[k], segB[k], nsegB[k] * 4, "sweep segments")) != SG_OK) goto done;
-        b->sweepB[k].chains = b->d_chB[k];
-        b->sweepB[k].seg = b->d_segB[k];
-        b->sweepB[k].nchains = nchB[k];
+        for (cls = 0; cls < SG_SWEEP_CLASSES; cls++) {
+            sg_sweep_tables *t = &b->sweepB[k][cls];
+            const int64_t hi = cls + 1 < SG_SWEEP_CLASSES ? first[cls + 1] : nchB[k];
+            t->chains = b->d_chB[k] + first[cls];
+            t->seg = b->d_segB[k];
+            t->nchains = hi - first[cls];
+            t->cap32 = t->cap64 = 0;
+            t->lmax_max = 0;
+            for (i = first[cls]; i < hi; i++) {
+                const int64_t e32 = chain_elems(&chB[k][i], 4), e64 = chain_elems(&chB[k][i], 8);
+                if (e32 > t->cap32) t->cap32 = e32;
+                if (e64 > t->cap64) t->cap64 = e64;
+                if (chB[k][i].lmax > t->lmax_max) t->lmax_max = chB[k][i].lmax;
+            }
+        }
     }
 
     /* evaluation: repack table over all grids, per-grid block sizes */
@@ -502,25 +541,39 @@ static int hier_launches(sg_batch *b, cudaStream_t st)
     int k, c, e;
     const int fp64 = b->precision == SG_HIER_FP64;
     if (b->has_sweep_grids) {
-        if (fp64) {
-            if ((e = sgk_widen(b->d_alpha, b->d_work, b->doff[b->ng], st)) != cudaSuccess) return bcuda((cudaError_t)e, "widen");
-            for (k = 0; k < SG_MAX_DIMS; k++) {
-                if (!b->sweepB[k].nchains) continue;
-                e = sgk_chain_smem_bytes(b->sweepB[k].cap64, 8) >= 0
-                        ? sgk_sweep_chains_f64(b->d_work, &b->sweepB[k], b->d_err, st)
-                        : sgk_sweep_gather_f64(b->d_work, &b->sweepB[k], st);
-                if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch FP64 sweep");
-            }
-            if ((e = sgk_narrow(b->d_work, b->d_alpha, b->doff[b->ng], st)) != cudaSuccess) return bcuda((cudaError_t)e, "narrow");
-        } else {
-            for (k = 0; k < SG_MAX_DIMS; k++) {
-                if (!b->sweepB[k].nchains) continue;
-                e = sgk_chain_smem_bytes(b->sweepB[k].cap32, 4) >= 0
-                        ? sgk_sweep_chains_f32(b->d_alpha, &b->sweepB[k], b->d_err, st)
-                        : sgk_sweep_gather_f32(b->d_alpha, &b->sweepB[k], st);
-                if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch FP32 sweep");
+        if (fp64 && (e = sgk_widen(b->d_alpha, b->d_work, b->doff[b->ng], st)) != cudaSuccess)
+            return bcuda((cudaError_t)e, "widen");
+        for (k = 0; k < SG_MAX_DIMS; k++) {
+            /* the size classes of sweep k are independent: fork them onto
+             * their own streams and join before sweep k+1 */
+            int any = 0;
+            for (c = 0; c < SG_SWEEP_CLASSES; c++) any |= b->sweepB[k][c].nchains > 0;
+            if (!any) continue;
+            BCU(cudaEventRecord(b->ev_fork, st), "cudaEventRecord");
+            for (c = 0; c < SG_SWEEP_CLASSES; c++) {
+                const sg_sweep_tables *t = &b->sweepB[k][c];
+                cudaStream_t cs = b->dst[1 + c];
+                if (!t->nchains) continue;
+                BCU(cudaStreamWaitEvent(cs, b->ev_fork, 0), "cudaStreamWaitEvent");
+                /* kernel: 2 gather; 3 (or 0 for the shortest chains) one warp
+                 * per chain; otherwise the staged chain kernel where it fits */
+                const int kern = b->hier_kernel[c] ? b->hier_kernel[c] : (c == SG_SWEEP_CLASSES - 1 ? 3 : 1);
+                const int64_t cap = fp64 ? t->cap64 : t->cap32;
+                const int eb = fp64 ? 8 : 4;
+                if (kern == 3 && sgk_small_smem_bytes(cap, eb) >= 0)
+                    e = fp64 ? sgk_sweep_small_f64(b->d_work, t, cs) : sgk_sweep_small_f32(b->d_alpha, t, cs);
+                else if (kern != 2 && sgk_chain_smem_bytes(cap, eb) >= 0)
+                    e = fp64 ? sgk_sweep_chains_f64(b->d_work, t, b->d_err, cs)
+                             : sgk_sweep_chains_f32(b->d_alpha, t, b->d_err, cs);
+                else
+                    e = fp64 ? sgk_sweep_gather_f64(b->d_work, t, cs) : sgk_sweep_gather_f32(b->d_alpha, t, cs);
+                if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch sweep");
+                BCU(cudaEventRecord(b->ev_d[1 + c], cs), "cudaEventRecord");
+                BCU(cudaStreamWaitEvent(st, b->ev_d[1 + c], 0), "cudaStreamWaitEvent");
             }
         }
+        if (fp64 && (e = sgk_narrow(b->d_work, b->d_alpha, b->doff[b->ng], st)) != cudaSuccess)
+            return bcuda((cudaError_t)e, "narrow");
     }
     /* after the sweeps: their FP64 round trip rewrites the whole buffer with
      * the (unchanged) nodal values of the shared-memory grids */
@@ -570,6 +623,7 @@ SG_API int sg_batch_hierarchize_async(sg_batch *b, void *stream)
     if ((r = enter(b, &prev)) != SG_OK) return r;
     if (b->precision == SG_HIER_FP64 && b->has_sweep_grids && !b->d_work)
         r = balloc(b, (void **)&b->d_work, b->doff[b->ng] * 8, "batch FP64 working values");
+    if (r == SG_OK) r = make_fork_streams(b);
     if (r == SG_OK) r = b->use_graph ? run_graph(&b->hier_graph, hier_launches, b, st) : hier_launches(b, st);
     b->eval_dirty = 1;
     leave(b, prev);
@@ -799,6 +853,56 @@ SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const fl
     for (k = 0; k <= SG_MAX_DIMS; k++)
         b->ppt_d[k] = (r == SG_OK && t[0][k] >= 0.0) ? (t[0][k] <= t[1][k] ? 1 : 2) : 0;
     b->eval_dirty = 1;
+    /* sweeps: per chain size class, the staged chain kernel or one warp per
+     * chain (both bit-identical); the values are saved and restored */
+    if (r == SG_OK && b->has_sweep_grids) {
+        float *saved = NULL;
+        const size_t vb = (size_t)b->doff[b->ng] * 4;
+        int c, kern;
+        if (b->precision == SG_HIER_FP64 && !b->d_work &&
+            (r = balloc(b, (void **)&b->d_work, b->doff[b->ng] * 8, "batch FP64 working values")) != SG_OK)
+            goto done;
+        if (cudaMalloc((void **)&saved, vb) != cudaSuccess) {
+            cudaGetLastError();
+            r = bfail(SG_ERR_NOMEM, "sg_batch_autotune: no device memory to save the values");
+            goto done;
+        }
+        if (cudaMemcpyAsync(saved, b->d_alpha, vb, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+            r = bfail(SG_ERR_CUDA, "sg_batch_autotune: save");
+        for (c = 0; c < SG_SWEEP_CLASSES && r == SG_OK; c++) {
+            double best = -1.0;
+            int best_k = 0, any = 0;
+            for (k = 0; k < SG_MAX_DIMS; k++) any |= b->sweepB[k][c].nchains > 0;
+            if (!any) continue;
+            for (kern = 1; kern <= 3 && r == SG_OK; kern += 2) {
+                b->hier_kernel[c] = kern;
+                for (rep = 0; rep < 3 && r == SG_OK; rep++) {
+                    if (cudaMemcpyAsync(b->d_alpha, saved, vb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+                        cudaEventRecord(e0, st) != cudaSuccess) {
+                        r = bfail(SG_ERR_CUDA, "sg_batch_autotune: sweep timing");
+                        break;
+                    }
+                    if ((r = hier_launches(b, st)) != SG_OK) break;
+                    if (cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+                        cudaEventElapsedTime(&el, e0, e1) != cudaSuccess) {
+                        r = bfail(SG_ERR_CUDA, "sg_batch_autotune: sweep timing");
+                        break;
+                    }
+                    if (rep > 0 && (best < 0.0 || el < best)) best = el, best_k = kern;
+                }
+            }
+            b->hier_kernel[c] = best_k;
+        }
+        if (cudaMemcpyAsync(b->d_alpha, saved, vb, cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+            cudaStreamSynchronize(st) != cudaSuccess) {
+            if (r == SG_OK) r = bfail(SG_ERR_CUDA, "sg_batch_autotune: restore");
+        }
+        cudaFree(saved);
+        if (b->hier_graph) {
+            cudaGraphExecDestroy(b->hier_graph);
+            b->hier_graph = NULL;
+        }
+    }
     if (ms)
         for (pi = 0; pi < 2; pi++)
             for (k = 0; k <= SG_MAX_DIMS; k++) ms[pi * (SG_MAX_DIMS + 1) + k] = t[pi][k];
@@ -830,6 +934,16 @@ SG_API int sg_batch_set_option(sg_batch *b, int option, int64_t value)
         if (value != 0 && value != 1) return bfail(SG_ERR_ARG, "SG_OPT_USE_GRAPH is 0 or 1");
         b->use_graph = (int)value;
         return SG_OK;
+    case SG_OPT_HIER_KERNEL: {
+        int c;
+        if (value < 0 || value > 3) return bfail(SG_ERR_ARG, "SG_OPT_HIER_KERNEL is 0, 1, 2 or 3");
+        for (c = 0; c < SG_SWEEP_CLASSES; c++) b->hier_kernel[c] = (int)value;
+        if (b->hier_graph) {
+            cudaGraphExecDestroy(b->hier_graph);
+            b->hier_graph = NULL;
+        }
+        return SG_OK;
+    }
     default:
         return bfail(SG_ERR_ARG, "option %d does not apply to batches", option);
     }

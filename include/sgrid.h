@@ -61,7 +61,8 @@ extern "C" {
 #define SG_OPT_EVAL_SORT 2      /* 1 (default): spatially order points on the GPU   */
                                 /* before evaluating; 0: evaluate in caller order    */
 #define SG_OPT_EVAL_PPT 3       /* points per thread in evaluate: 0 = auto, 1, 2     */
-#define SG_OPT_HIER_KERNEL 5    /* 0 = auto, 1 = shared-memory chains, 2 = gather    */
+#define SG_OPT_HIER_KERNEL 5    /* 0 = auto, 1 = shared-memory chains, 2 = gather,   */
+                                /* 3 = one warp per chain (batches only)            */
 #define SG_OPT_PROFILE 6        /* 1: record CUDA events around each phase            */
 #define SG_OPT_USE_GRAPH 7      /* batches: 1 (default) capture launches in a CUDA graph */
 
@@ -229,12 +230,15 @@ int sg_batch_hierarchize(sg_batch *batch);
 int sg_batch_evaluate_device(sg_batch *batch, const int64_t *point_offsets, const float *coord_mat,
                              float *out, void *stream);
 int sg_batch_sync(sg_batch *batch, void *stream);
-/* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH */
+/* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH, SG_OPT_HIER_KERNEL (sweeps) */
 int sg_batch_set_option(sg_batch *batch, int option, int64_t value);
-/* Autotuner for the batched evaluation (no reference counterpart): times
- * each dimension's launch over the caller's points at 1 and at 2 points per
- * thread and keeps the faster per dimension (results do not change).  Until
- * the next SG_OPT_EVAL_PPT setting, which replaces it.  ms (optional,
+/* Autotuner for batches (no reference counterpart): times each
+ * dimension's evaluation launch over the caller's points at 1 and at 2
+ * points per thread and keeps the faster per dimension, and times the
+ * hierarchization with each chain size class on the staged chain kernel and
+ * on one warp per chain and keeps the faster per class (the values are
+ * saved and restored).  Results do not change.  An SG_OPT_EVAL_PPT or
+ * SG_OPT_HIER_KERNEL setting replaces the tuned choice.  ms (optional,
  * 2*(SG_MAX_DIMS+1) entries): [ppt-1][d] launch ms, -1 where no grid has d. */
 int sg_batch_autotune(sg_batch *batch, const int64_t *point_offsets, const float *coord_mat, float *out,
                       void *stream, double *ms);

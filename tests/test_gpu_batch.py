@@ -24,10 +24,13 @@ def _batch(shapes):
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-@pytest.mark.parametrize("graph", [1, 0])
-def test_batch_hierarchize_matches_single_grids(cuda, precision, graph):
+@pytest.mark.parametrize("graph,kernel", [(1, 0), (0, 0), (1, 1), (1, 3)])
+def test_batch_hierarchize_matches_single_grids(cuda, precision, graph, kernel):
+    # kernel 0: auto (short chains one warp per chain), 1: staged chains
+    # everywhere, 3: one warp per chain wherever the chains fit
     b = _batch(MIXED)
     b.set_option(_lib.SG_OPT_USE_GRAPH, graph)
+    b.set_option(_lib.SG_OPT_HIER_KERNEL, kernel)
     b.set_option(_lib.SG_OPT_HIER_PRECISION, _lib.SG_HIER_FP64 if precision == "fp64" else _lib.SG_HIER_FP32)
     vals = inputs.uniform01(77, b.num_values) * 2 - 1
     for rep in range(2):  # the second run replays the graph
@@ -112,7 +115,10 @@ def test_batch_autotune_keeps_results(cuda):
     b.evaluate_device(po, coords, out)
     b.sync()
     before = out.cpu().numpy().copy()
+    surplus = b.get_values()
     ms = b.autotune(po, coords, out)
+    # the sweep tuning hierarchizes saved copies: the values are restored
+    assert np.array_equal(b.get_values().view(np.uint32), surplus.view(np.uint32))
     dims_present = sorted({d for d, _, _ in MIXED})
     for d in range(1, _lib.SG_MAX_DIMS + 1):
         if d in dims_present:
@@ -124,3 +130,7 @@ def test_batch_autotune_keeps_results(cuda):
         b.evaluate_device(po, coords, out)
         b.sync()
     assert np.array_equal(out.cpu().numpy().view(np.uint32), before.view(np.uint32))
+    # the tuned sweep kernels give the same surpluses
+    b.set_values(vals)
+    b.hierarchize()
+    assert np.array_equal(b.get_values().view(np.uint32), surplus.view(np.uint32))
