@@ -149,6 +149,42 @@ __global__ void k_sort_scatter(const float *__restrict__ coords, int64_t n, int 
     }
 }
 
+/* Batched form: CTA b handles 256 points of grid items[b].x from local
+ * point items[b].y; the key of a point is its grid's bin base plus its
+ * Morton cell, so the bins of one grid are contiguous and, after one scan
+ * over all bins, a grid's points land inside its own point range. */
+__global__ void __launch_bounds__(256) k_bsort_keys(const float *__restrict__ coords,
+                                                    const sg_bsort_grid *__restrict__ grids,
+                                                    const int2 *__restrict__ items, uint32_t *__restrict__ keys,
+                                                    uint32_t *__restrict__ hist)
+{
+    const int2 it = items[blockIdx.x];
+    const sg_bsort_grid G = grids[it.x];
+    const int64_t i = (int64_t)it.y + threadIdx.x;
+    if (i >= G.m) return;
+    float x[SG_MAX_DIMS];
+    for (int k = 0; k < G.d; ++k) x[k] = coords[G.coff + i * G.d + k];
+    const uint32_t key = G.bin_base + morton_key(x, G.d, G.kb);
+    keys[G.pt_off + i] = key;
+    atomicAdd(hist + key, 1u);
+}
+
+__global__ void __launch_bounds__(256) k_bsort_scatter(const float *__restrict__ coords,
+                                                       const sg_bsort_grid *__restrict__ grids,
+                                                       const int2 *__restrict__ items,
+                                                       const uint32_t *__restrict__ keys,
+                                                       uint32_t *__restrict__ cursor, float *__restrict__ sorted,
+                                                       int32_t *__restrict__ perm)
+{
+    const int2 it = items[blockIdx.x];
+    const sg_bsort_grid G = grids[it.x];
+    const int64_t i = (int64_t)it.y + threadIdx.x;
+    if (i >= G.m) return;
+    const int64_t pos = (int64_t)atomicAdd(cursor + keys[G.pt_off + i], 1u) - G.pt_off; /* local position */
+    for (int k = 0; k < G.d; ++k) sorted[G.coff + pos * G.d + k] = coords[G.coff + i * G.d + k];
+    perm[G.pt_off + pos] = (int32_t)i;
+}
+
 int sort_key_bits(int64_t n, int d)
 {
     int kb = 0;
@@ -274,6 +310,33 @@ int64_t sgk_sort_scratch_bytes(int64_t num_evals, int d)
     const int64_t bins = (int64_t)1 << sort_key_bits(num_evals, d);
     (void)d;
     return (num_evals + bins + scan_tmp_words(bins)) * 4 + 256;
+}
+
+int sgk_batch_sort_bits(int64_t m, int d) { return sort_key_bits(m, d); }
+
+int64_t sgk_batch_sort_scratch_bytes(int64_t npts, int64_t nbins)
+{
+    return (npts + nbins + scan_tmp_words(nbins)) * 4 + 256;
+}
+
+int sgk_batch_sort_points(const float *coords, const sg_bsort_grid *grids, const int32_t *items, int nitems,
+                          int64_t npts, int64_t nbins, void *scratch, float *sorted, int32_t *perm, void *stream)
+{
+    if (nitems <= 0 || npts <= 0) return cudaSuccess;
+    cudaStream_t st = (cudaStream_t)stream;
+    uint32_t *keys = (uint32_t *)scratch;
+    uint32_t *hist = keys + npts;
+    uint32_t *tmp = hist + nbins;
+    const int2 *it = reinterpret_cast<const int2 *>(items);
+    cudaError_t e = cudaMemsetAsync(hist, 0, (size_t)nbins * 4, st);
+    if (e != cudaSuccess) return e;
+    k_bsort_keys<<<nitems, 256, 0, st>>>(coords, grids, it, keys, hist);
+    sgk_count(1);
+    int r = scan_exclusive(hist, nbins, tmp, st);
+    if (r != cudaSuccess) return r;
+    k_bsort_scatter<<<nitems, 256, 0, st>>>(coords, grids, it, keys, hist, sorted, perm);
+    sgk_count(1);
+    return cudaGetLastError();
 }
 
 int sgk_sort_points(const float *coords, int64_t n, int d, void *scratch, float *sorted,

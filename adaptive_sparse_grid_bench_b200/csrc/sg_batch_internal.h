@@ -52,6 +52,15 @@ struct sg_batch {
     int64_t *eval_pt_off;
     const float *eval_coords;
     float *eval_out;
+    int sort;                        /* spatial ordering of each grid's points (default 1) */
+    int eval_sort;                   /* the setting the current plan was built for */
+    sg_bsort_grid *d_sgrids;         /* sort: per-grid geometry                  */
+    int32_t *d_sitems;               /* sort: CTA items, 256 points each          */
+    int nsitems;
+    int64_t sort_npts, sort_nbins, sort_bytes;
+    void *d_sscratch;                /* sort: keys, histogram, scan               */
+    float *d_sorted;                 /* sorted coordinates                         */
+    int32_t *d_perm;                 /* sorted position -> caller's local index    */
     int ppt_d[SG_MAX_DIMS + 1];      /* points per thread per dimension (0: ppt) */
     int eval_ppt_d[SG_MAX_DIMS + 1]; /* the setting the current plan was built for */
     int *order;                      /* grids by dimension, most subspaces first */

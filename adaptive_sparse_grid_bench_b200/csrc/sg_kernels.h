@@ -137,6 +137,23 @@ int64_t sgk_sort_scratch_bytes(int64_t num_evals, int d);
 int sgk_sort_points(const float *coords, int64_t num_evals, int d, void *scratch,
                     float *sorted, int32_t *perm, void *stream);
 
+/* Spatial ordering of a batch's points, each grid's points among
+ * themselves: per grid its point count m, point offset, coordinate offset,
+ * dimension, Morton key bits (sgk_batch_sort_bits) and first bin; items
+ * (device, 2 ints per CTA) = (grid, first local point), 256 points per CTA.
+ * Writes sorted coordinates at the same offsets and perm[pt_off + sorted
+ * local position] = caller's local index.  scratch: device bytes of at
+ * least sgk_batch_sort_scratch_bytes(total points, total bins). */
+typedef struct sg_bsort_grid {
+    int64_t m, pt_off, coff;
+    uint32_t bin_base;
+    int d, kb;
+} sg_bsort_grid;
+int sgk_batch_sort_bits(int64_t m, int d);
+int64_t sgk_batch_sort_scratch_bytes(int64_t npts, int64_t nbins);
+int sgk_batch_sort_points(const float *coords, const sg_bsort_grid *grids, const int32_t *items, int nitems,
+                          int64_t npts, int64_t nbins, void *scratch, float *sorted, int32_t *perm, void *stream);
+
 /* Batched bijection on the device. */
 int sgk_idx2gp(const sg_layout *L, const int64_t *index, int *levels, int *indices,
                int64_t count, void *stream);

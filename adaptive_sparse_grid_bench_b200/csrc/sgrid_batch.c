@@ -91,6 +91,7 @@ SG_API int sg_batch_create(int num_grids, const int *dims, const int *levels, co
     b->ppt = 2;
     b->precision = SG_HIER_FP32;
     b->use_graph = 1;
+    b->sort = 1;
     *out = b;
     return SG_OK;
 }
@@ -114,6 +115,16 @@ static void free_dev(sg_batch *b)
         cudaFree(b->d_chB[k]);
         cudaFree(b->d_segB[k]);
     }
+    cudaFree(b->d_sgrids);
+    cudaFree(b->d_sitems);
+    cudaFree(b->d_sscratch);
+    cudaFree(b->d_sorted);
+    cudaFree(b->d_perm);
+    b->d_sgrids = NULL;
+    b->d_sitems = NULL;
+    b->d_sscratch = NULL;
+    b->d_sorted = NULL;
+    b->d_perm = NULL;
     cudaFree(b->d_eval_args);
     cudaFree(b->d_items);
     cudaFree(b->d_err);
@@ -668,11 +679,84 @@ static int cmp_dim_then_subspaces(const void *x, const void *y, void *ctx)
     return *(const int *)x - *(const int *)y;
 }
 
+/* Spatial ordering of every grid's points (among themselves): per-grid
+ * geometry, CTA items and buffers; points the evaluation arguments at the
+ * sorted coordinates and the permutation. */
+static int plan_sort(sg_batch *b, const int64_t *pt_off)
+{
+    sg_bsort_grid *sg = NULL;
+    int32_t *items = NULL;
+    int64_t coff = 0, nbins = 0, ni = 0, cap = 0, ncoord = 0, npts = pt_off[b->ng];
+    int g, r = SG_OK;
+    const int64_t before = b->dev_bytes;
+    b->dev_bytes -= b->sort_bytes;
+    cudaFree(b->d_sgrids);
+    cudaFree(b->d_sitems);
+    cudaFree(b->d_sscratch);
+    cudaFree(b->d_sorted);
+    cudaFree(b->d_perm);
+    b->d_sgrids = NULL;
+    b->d_sitems = NULL;
+    b->d_sscratch = NULL;
+    b->d_sorted = NULL;
+    b->d_perm = NULL;
+    b->nsitems = 0;
+    for (g = 0; g < b->ng; g++) {
+        cap += (pt_off[g + 1] - pt_off[g] + 255) / 256;
+        ncoord += (pt_off[g + 1] - pt_off[g]) * b->L[g].d;
+    }
+    sg = (sg_bsort_grid *)malloc(sizeof(sg_bsort_grid) * (size_t)b->ng);
+    items = (int32_t *)malloc(sizeof(int32_t) * 2 * (size_t)(cap > 0 ? cap : 1));
+    if (!sg || !items) {
+        r = bfail(SG_ERR_NOMEM, "out of host memory");
+        goto out;
+    }
+    for (g = 0; g < b->ng; g++) {
+        const int64_t m = pt_off[g + 1] - pt_off[g];
+        int64_t p;
+        sg[g].m = m;
+        sg[g].pt_off = pt_off[g];
+        sg[g].coff = coff;
+        sg[g].d = b->L[g].d;
+        sg[g].kb = sgk_batch_sort_bits(m, b->L[g].d);
+        sg[g].bin_base = (uint32_t)nbins;
+        nbins += (int64_t)1 << sg[g].kb;
+        coff += m * b->L[g].d;
+        for (p = 0; p < m; p += 256) {
+            items[2 * ni] = g;
+            items[2 * ni + 1] = (int32_t)p;
+            ni++;
+        }
+    }
+    if (nbins >= ((int64_t)1 << 31)) {
+        r = bfail(SG_ERR_RANGE, "sg_batch_evaluate: too many sort bins");
+        goto out;
+    }
+    if ((r = upload(b, (void **)&b->d_sgrids, sg, b->ng * (int64_t)sizeof(sg_bsort_grid), "sort geometry")) != SG_OK ||
+        (r = upload(b, (void **)&b->d_sitems, items, ni * 8, "sort items")) != SG_OK ||
+        (r = balloc(b, &b->d_sscratch, sgk_batch_sort_scratch_bytes(npts, nbins), "sort scratch")) != SG_OK ||
+        (r = balloc(b, (void **)&b->d_sorted, ncoord * 4, "sorted coordinates")) != SG_OK ||
+        (r = balloc(b, (void **)&b->d_perm, npts * 4, "sort permutation")) != SG_OK)
+        goto out;
+    b->nsitems = (int)ni;
+    b->sort_bytes = b->dev_bytes - before + b->sort_bytes;
+    b->sort_npts = npts;
+    b->sort_nbins = nbins;
+    for (g = 0; g < b->ng; g++) {
+        b->h_eval_args[g].coords = b->d_sorted + sg[g].coff;
+        b->h_eval_args[g].perm = b->d_perm + pt_off[g];
+    }
+out:
+    free(sg);
+    free(items);
+    return r;
+}
+
 static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, float *out)
 {
     int g, k, r, q;
     int64_t coff = 0, ni = 0, cap_items = 0;
-    int same = b->h_eval_args && b->eval_coords == coords && b->eval_out == out;
+    int same = b->h_eval_args && b->eval_coords == coords && b->eval_out == out && b->eval_sort == b->sort;
     for (k = 0; same && k <= SG_MAX_DIMS; k++) same = b->eval_ppt_d[k] == ppt_of(b, k);
     for (g = 0; same && g <= b->ng; g++) same = b->eval_pt_off[g] == pt_off[g];
     if (same) return SG_OK;
@@ -726,6 +810,7 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
         sgk_fill_eval_args(&p, coords + coff, NULL, out + pt_off[g], pt_off[g + 1] - pt_off[g], &b->h_eval_args[g]);
         coff += (pt_off[g + 1] - pt_off[g]) * L->d;
     }
+    if (b->sort && (r = plan_sort(b, pt_off)) != SG_OK) return r;
     /* items grouped by dimension, grids with the most subspaces first (their
      * CTAs are the longest) */
     for (k = 1; k <= SG_MAX_DIMS; k++) {
@@ -756,6 +841,7 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
     b->eval_coords = coords;
     b->eval_out = out;
     for (k = 0; k <= SG_MAX_DIMS; k++) b->eval_ppt_d[k] = ppt_of(b, k);
+    b->eval_sort = b->sort;
     return SG_OK;
 }
 
@@ -776,6 +862,10 @@ static int make_fork_streams(sg_batch *b)
 static int eval_launches(sg_batch *b, cudaStream_t st)
 {
     int k, e;
+    if (b->sort && (e = sgk_batch_sort_points(b->eval_coords, b->d_sgrids, b->d_sitems, b->nsitems, b->sort_npts,
+                                              b->sort_nbins, b->d_sscratch, b->d_sorted, b->d_perm, st)) !=
+                       cudaSuccess)
+        return bcuda((cudaError_t)e, "batch spatial ordering");
     if ((e = sgk_repack(b->d_alpha, b->d_blk, b->d_repack, b->nrepack, st)) != cudaSuccess)
         return bcuda((cudaError_t)e, "batch repack");
     BCU(cudaEventRecord(b->ev_fork, st), "cudaEventRecord");
@@ -831,6 +921,11 @@ SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const fl
     for (pi = 0; pi < 2 && r == SG_OK; pi++) {
         for (k = 0; k <= SG_MAX_DIMS; k++) b->ppt_d[k] = pi + 1;
         if ((r = plan_eval(b, point_offsets, coords, out)) != SG_OK) break;
+        if (b->sort && sgk_batch_sort_points(coords, b->d_sgrids, b->d_sitems, b->nsitems, b->sort_npts, b->sort_nbins,
+                                             b->d_sscratch, b->d_sorted, b->d_perm, st) != cudaSuccess) {
+            r = bfail(SG_ERR_CUDA, "sg_batch_autotune: spatial ordering");
+            break;
+        }
         if (sgk_repack(b->d_alpha, b->d_blk, b->d_repack, b->nrepack, st) != cudaSuccess) {
             r = bfail(SG_ERR_CUDA, "sg_batch_autotune: repack");
             break;
@@ -933,6 +1028,10 @@ SG_API int sg_batch_set_option(sg_batch *b, int option, int64_t value)
     case SG_OPT_USE_GRAPH:
         if (value != 0 && value != 1) return bfail(SG_ERR_ARG, "SG_OPT_USE_GRAPH is 0 or 1");
         b->use_graph = (int)value;
+        return SG_OK;
+    case SG_OPT_EVAL_SORT:
+        if (value != 0 && value != 1) return bfail(SG_ERR_ARG, "SG_OPT_EVAL_SORT is 0 or 1");
+        b->sort = (int)value;
         return SG_OK;
     case SG_OPT_HIER_KERNEL: {
         int c;

@@ -230,7 +230,8 @@ int sg_batch_hierarchize(sg_batch *batch);
 int sg_batch_evaluate_device(sg_batch *batch, const int64_t *point_offsets, const float *coord_mat,
                              float *out, void *stream);
 int sg_batch_sync(sg_batch *batch, void *stream);
-/* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH, SG_OPT_HIER_KERNEL (sweeps) */
+/* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH, SG_OPT_HIER_KERNEL (sweeps),
+ * SG_OPT_EVAL_SORT (1, default: each grid's points spatially ordered on the GPU) */
 int sg_batch_set_option(sg_batch *batch, int option, int64_t value);
 /* Autotuner for batches (no reference counterpart): times each
  * dimension's evaluation launch over the caller's points at 1 and at 2

@@ -46,11 +46,12 @@ def test_batch_hierarchize_matches_single_grids(cuda, precision, graph, kernel):
         assert np.array_equal(b.grid_values(got, g).view(np.uint32), want.view(np.uint32)), f"grid {g} {d} {n}"
 
 
-@pytest.mark.parametrize("ppt", [1, 2])
-def test_batch_evaluate_matches_single_grids(cuda, ppt):
+@pytest.mark.parametrize("ppt,sort", [(1, 1), (2, 1), (2, 0)])
+def test_batch_evaluate_matches_single_grids(cuda, ppt, sort):
     import torch
     b = _batch(MIXED)
     b.set_option(_lib.SG_OPT_EVAL_PPT, ppt)
+    b.set_option(_lib.SG_OPT_EVAL_SORT, sort)
     vals = inputs.uniform01(78, b.num_values) * 2 - 1
     b.set_values(vals)
     b.hierarchize()
