@@ -34,6 +34,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 D, NLEV, M_EVAL, SEED = 10, 10, 1 << 24, 1
+# DRAM bytes (read + write) of one k_evaluate launch of the default workload
+# (2^24 points), from one ncu capture of this bench; summary and command in
+# profiles/k_evaluate_d10n10_2p24pts_dram.md
+EVAL_TRAFFIC_2P24 = 2.02e9 + 0.553e9
 WORKLOAD = "regular sparse grid d=10 n=10 (N=32,978,945), f=exp(-|x|^2), hierarchize + evaluate 2^24 uniform points"
 
 
@@ -368,7 +372,9 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None):
         "evaluate": {"ms": eval_ms, "sort_ms": statistics.mean(t_sort), "evals_per_s": m / (eval_ms / 1e3),
                      "pairs_per_s": m * S / (eval_ms / 1e3)},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "kernel": "k_evaluate", "peak_source": peak_src,
+                     "traffic": (EVAL_TRAFFIC_2P24 if wl["name"] == WORKLOAD and m == M_EVAL else None),
+                     "traffic_source": "ncu dram__bytes_read+write of one full launch (profiles/)",
+                     "kernel": "k_evaluate", "peak_source": peak_src,
                      "bytes": "4*(S+d+1) per query point (cache-served surplus reads counted)"},
         "e2e": e2e,
         "gpu_launches": int(launches),
