@@ -16,7 +16,14 @@ inside the timed region.  Inputs (132 MB grid + 671 MB points per rank) are
 larger than the 126 MB L2, so no flush is needed between steps.
 `--impl reference` times the reference's own C/OpenMP code
 (omp_hierarchize3 + omp_evaluate5, compiled in place into oracle/_ref) on the
-host cores, on a bounded sample of the same workload.
+host cores, on a bounded sample of the same workload.  Before timing, the
+library's autotuner picks the evaluation and sweep settings on the bench's
+own buffers (no setting changes a result).
+
+Other workloads (`--workload`): `adaptive` (the limits-adaptive d=6 grid
+refined by sg_refine, 2^22 points), `batched` (4096 grids of mixed d and n
+in one batch), `served` (the serving loop under a Poisson request sweep,
+with p50/p99 latency and the plain one-call-per-request comparison).
 """
 from __future__ import annotations
 
