@@ -139,7 +139,10 @@ int sgk_sort_points(const float *coords, int64_t num_evals, int d, void *scratch
 
 /* Spatial ordering of a batch's points, each grid's points among
  * themselves: per grid its point count m, point offset, coordinate offset,
- * dimension, Morton key bits (sgk_batch_sort_bits) and first bin; items
+ * dimension, Morton key bits (sgk_batch_sort_bits) and first bin.  The
+ * grids' bins must be in the order of their point offsets and the point
+ * offsets must be the running sum of the m of the grids listed (the sort's
+ * positions are counted over exactly these points); items
  * (device, 2 ints per CTA) = (grid, first local point), 256 points per CTA.
  * Writes sorted coordinates at the same offsets and perm[pt_off + sorted
  * local position] = caller's local index.  scratch: device bytes of at
