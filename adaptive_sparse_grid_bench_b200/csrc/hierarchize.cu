@@ -427,16 +427,21 @@ int launch_chains(T *a, const sg_sweep_tables *t, int *err, void *stream)
 
 /* Small chains (the many short chains of batched grids): one warp per
  * chain.  The warp loads the chain's segments into its own shared-memory
- * buffer with plain coalesced loads (no bulk copies, barriers or CTA-wide
+ * buffer with coalesced 16-byte loads (no bulk copies, barriers or CTA-wide
  * synchronisation, whose fixed cost dominates a chain of a few hundred
- * values), then writes each updated point straight to global memory: the
- * updates read only the pre-sweep values in the buffer, with the same
- * arithmetic as k_sweep_chains, so results are bit-identical. */
+ * values), then writes the updated points straight to global memory, four
+ * FP32 values (two FP64) per lane and 16-byte store wherever 2^sigma holds
+ * a whole group: the updates read only the pre-sweep values in the buffer,
+ * with the same arithmetic as k_sweep_chains, so results are bit-identical.
+ * The one-value-per-lane form spent most of its time issuing index
+ * arithmetic (issue-bound at a fifth of the DRAM bandwidth). */
 template <typename T>
 __global__ void __launch_bounds__(256) k_sweep_small(T *__restrict__ a, const sg_chain *__restrict__ chains,
                                                      const uint32_t *__restrict__ seg, int nch, int cap)
 {
     constexpr int A = 16 / sizeof(T);
+    using V = typename Vec<T>::type;
+    constexpr int W = Vec<T>::W;
     extern __shared__ __align__(16) unsigned char smem_small[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     T *buf = reinterpret_cast<T *>(smem_small) + (size_t)w * cap;
@@ -445,17 +450,47 @@ __global__ void __launch_bounds__(256) k_sweep_small(T *__restrict__ a, const sg
      * warp-uniform */
     for (int c = blockIdx.x * (blockDim.x >> 5) + w; c < nch; c += nw) {
         const sg_chain ch = chains[c];
-        for (int j = 0; j <= ch.lmax; ++j) {
-            const int n = 1 << (ch.sigma + j);
+        const int sigma = ch.sigma, lo = ch.lo, lmax = ch.lmax;
+        /* a subspace of 2^s values starts on a multiple of 2^s in the
+         * group-aligned layout, so every segment of at least 16 bytes moves
+         * with 16-byte loads; its shared-memory slot is 16-byte aligned too
+         * (cap and the segment starts are multiples of A) */
+        for (int j = 0; j <= lmax; ++j) {
+            const int n = 1 << (sigma + j);
             const T *src = a + seg[ch.seg + j];
-            T *dst = buf + seg_soff<A>(ch.sigma, j);
-            for (int p = lane; p < n; p += 32) dst[p] = src[p];
+            T *dst = buf + seg_soff<A>(sigma, j);
+            if (n >= W) {
+                for (int v = lane; v < n / W; v += 32)
+                    reinterpret_cast<V *>(dst)[v] = reinterpret_cast<const V *>(src)[v];
+            } else if (lane < n) {
+                dst[lane] = src[lane];
+            }
         }
         __syncwarp();
-        for (int j = 1; j <= ch.lmax; ++j) {
-            const int n = 1 << (ch.sigma + j);
-            T *out = a + seg[ch.seg + j];
-            for (int p = lane; p < n; p += 32) out[p] = chain_point<T, A>(buf, ch.sigma, ch.lo, j, p);
+        /* updated points: segments 1..lmax flattened, segment j starting at
+         * q = 2^sigma (2^j - 2); W at a time when a pole group holds W
+         * consecutive values, with the arithmetic of k_sweep_chains */
+        const int U = (((2 << lmax) - 2) << sigma);
+        if ((1 << sigma) >= W) {
+            for (int v = lane; v < U / W; v += 32) {
+                const int q = v * W;
+                const int j = 31 - __clz((q >> sigma) + 2);
+                const int p = q - (((1 << j) - 2) << sigma);
+                V o;
+                if constexpr (W == 4) {
+                    o = chain_group4(buf, sigma, lo, j, p);
+                } else {
+                    o = make_double2(chain_point<T, A>(buf, sigma, lo, j, p),
+                                     chain_point<T, A>(buf, sigma, lo, j, p + 1));
+                }
+                *reinterpret_cast<V *>(a + seg[ch.seg + j] + p) = o;
+            }
+        } else {
+            for (int q = lane; q < U; q += 32) {
+                const int j = 31 - __clz((q >> sigma) + 2);
+                const int p = q - (((1 << j) - 2) << sigma);
+                a[seg[ch.seg + j] + p] = chain_point<T, A>(buf, sigma, lo, j, p);
+            }
         }
         __syncwarp();
     }
