@@ -11,6 +11,7 @@
 
 #define SG_BATCH_CLASSES 4 /* size classes of the shared-memory hierarchization */
 #define SG_SWEEP_CLASSES 3 /* chain size classes of the batched sweeps          */
+#define SG_SWEEP_STREAMS 4 /* concurrent streams of grouped sweeps             */
 
 struct sg_batch {
     int ng;
@@ -37,9 +38,16 @@ struct sg_batch {
     uint32_t *d_smem_seg;
     /* chain-sweep path */
     int has_sweep_grids;
-    /* chains of sweep k sorted by size, in SG_SWEEP_CLASSES classes that
-     * launch with their own CTA size and shared-memory stages */
-    sg_sweep_tables sweepB[SG_MAX_DIMS][SG_SWEEP_CLASSES];
+    /* sweep groups: consecutive runs of sweep grids holding at most
+     * sweep_group values (0: the whole batch is one group).  Grouped, all d
+     * sweeps of a group run back to back on one of SG_SWEEP_STREAMS
+     * streams, so the group's values stay in L2 between its sweeps.  Per
+     * group, the chains of sweep k are sorted by size into SG_SWEEP_CLASSES
+     * classes that launch with their own CTA size and shared-memory stages:
+     * table (q, k, c) is sweepG[(q * SG_MAX_DIMS + k) * SG_SWEEP_CLASSES + c] */
+    int64_t sweep_group;
+    int ngroups;
+    sg_sweep_tables *sweepG;
     sg_chain *d_chB[SG_MAX_DIMS];
     uint32_t *d_segB[SG_MAX_DIMS];
     /* evaluation */
@@ -69,6 +77,7 @@ struct sg_batch {
     cudaStream_t dst[SG_MAX_DIMS + 1];
     cudaEvent_t ev_fork, ev_d[SG_MAX_DIMS + 1];
     cudaGraphExec_t hier_graph, eval_graph;
+    int64_t hier_graph_kernels, eval_graph_kernels; /* kernel launches captured in each graph */
 };
 
 /* Sets the calling thread's sg_last_error() text (sgrid.c). */

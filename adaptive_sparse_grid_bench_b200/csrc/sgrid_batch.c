@@ -24,6 +24,11 @@
 
 #define SG_API __attribute__((visibility("default")))
 
+/* values per sweep group (SG_OPT_SWEEP_GROUP): measured on 4096 mixed grids
+ * (5.1e8 values), smaller groups lose more to launch latency than they
+ * gain from L2 */
+#define SG_SWEEP_GROUP_DEFAULT (1 << 23)
+
 /* size classes of the shared-memory path (bytes of the larger of FP32/FP64) */
 static const int64_t k_class_bytes[SG_BATCH_CLASSES] = {8 * 1024, 32 * 1024, 96 * 1024, SG_SMEM_GRID_MAX_BYTES};
 
@@ -92,6 +97,7 @@ SG_API int sg_batch_create(int num_grids, const int *dims, const int *levels, co
     b->precision = SG_HIER_FP32;
     b->use_graph = 1;
     b->sort = 1;
+    b->sweep_group = SG_SWEEP_GROUP_DEFAULT;
     *out = b;
     return SG_OK;
 }
@@ -114,7 +120,12 @@ static void free_dev(sg_batch *b)
     for (k = 0; k < SG_MAX_DIMS; k++) {
         cudaFree(b->d_chB[k]);
         cudaFree(b->d_segB[k]);
+        b->d_chB[k] = NULL;
+        b->d_segB[k] = NULL;
     }
+    free(b->sweepG);
+    b->sweepG = NULL;
+    b->ngroups = 0;
     cudaFree(b->d_sgrids);
     cudaFree(b->d_sitems);
     cudaFree(b->d_sscratch);
@@ -248,6 +259,9 @@ static int materialize(sg_batch *b)
     int64_t nchB[SG_MAX_DIMS], nsegB[SG_MAX_DIMS], capchB[SG_MAX_DIMS], capsegB[SG_MAX_DIMS];
     sg_repack *rp = NULL;
     int64_t nrp = 0;
+    int64_t (*gfirst)[SG_MAX_DIMS] = NULL; /* first chain of each sweep group per sweep, ngroups+1 rows */
+    int ngr = 0, capgr = 0, q;
+    int64_t gacc = 0;
     if (b->dev >= 0) return SG_OK;
     memset(chB, 0, sizeof(chB));
     memset(segB, 0, sizeof(segB));
@@ -345,11 +359,25 @@ static int materialize(sg_batch *b)
     if ((r = upload(b, (void **)&b->d_smem_chains, sch, nsch * (int64_t)sizeof(sg_chain), "batch chains")) != SG_OK) goto done;
     if ((r = upload(b, (void **)&b->d_smem_seg, sseg, nsseg * 4, "batch segments")) != SG_OK) goto done;
 
-    /* chain-sweep path: sweep k of every other grid in one launch */
+    /* chain-sweep path: the other grids, in sweep groups of consecutive
+     * grids; sweep k of every grid of a group in one launch per class */
     for (g = 0; g < b->ng; g++) {
         const sg_layout *L = &b->L[g];
         if (smem_class(L) >= 0) continue;
         b->has_sweep_grids = 1;
+        if (ngr == 0 || (b->sweep_group > 0 && gacc > 0 && gacc + L->Npad > b->sweep_group)) {
+            if (ngr + 1 >= capgr) {
+                void *ng2;
+                capgr = capgr ? 2 * capgr : 64;
+                ng2 = realloc(gfirst, (size_t)capgr * sizeof(*gfirst));
+                if (!ng2) { r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
+                gfirst = (int64_t(*)[SG_MAX_DIMS])ng2;
+            }
+            for (k = 0; k < SG_MAX_DIMS; k++) gfirst[ngr][k] = nchB[k];
+            ngr++;
+            gacc = 0;
+        }
+        gacc += L->Npad;
         for (k = 0; k < L->d; k++) {
             sg_chain *ch = NULL;
             uint32_t *sgo = NULL;
@@ -375,34 +403,50 @@ static int materialize(sg_batch *b)
             free(sgo);
         }
     }
+    if (ngr == 0) ngr = 1; /* no sweep grids: one empty group */
+    if (!gfirst) {
+        gfirst = (int64_t(*)[SG_MAX_DIMS])calloc(2, sizeof(*gfirst));
+        if (!gfirst) { r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
+    }
+    for (k = 0; k < SG_MAX_DIMS; k++) gfirst[ngr][k] = nchB[k];
+    b->ngroups = ngr;
+    b->sweepG = (sg_sweep_tables *)calloc((size_t)ngr * SG_MAX_DIMS * SG_SWEEP_CLASSES, sizeof(sg_sweep_tables));
+    if (!b->sweepG) { r = bfail(SG_ERR_NOMEM, "out of host memory"); goto done; }
     for (k = 0; k < SG_MAX_DIMS; k++) {
-        int64_t i, first[SG_SWEEP_CLASSES + 1];
-        int cls;
-        /* largest chains first, then split by the CTA size they need */
-        if (nchB[k] > 1) qsort(chB[k], (size_t)nchB[k], sizeof(sg_chain), cmp_chain_desc);
-        /* classes are contiguous (sorted by size): count, then prefix sums */
-        for (cls = 0; cls <= SG_SWEEP_CLASSES; cls++) first[cls] = 0;
-        for (i = 0; i < nchB[k]; i++) {
-            const int64_t e32 = chain_elems(&chB[k][i], 4);
-            first[1 + (e32 > 256 * 12 ? 0 : (e32 > 128 * 12 ? 1 : 2))]++;
+        if ((r = upload(b, (void **)&b->d_segB[k], segB[k], nsegB[k] * 4, "sweep segments")) != SG_OK) goto done;
+        /* per group: largest chains first, then split by the CTA size they
+         * need (the chains of a group are contiguous: its grids are) */
+        for (q = 0; q < ngr; q++) {
+            const int64_t lo = gfirst[q][k], cnt = gfirst[q + 1][k] - gfirst[q][k];
+            if (cnt > 1) qsort(chB[k] + lo, (size_t)cnt, sizeof(sg_chain), cmp_chain_desc);
         }
-        for (cls = 1; cls <= SG_SWEEP_CLASSES; cls++) first[cls] += first[cls - 1];
         if ((r = upload(b, (void **)&b->d_chB[k], chB[k], nchB[k] * (int64_t)sizeof(sg_chain), "sweep chains")) != SG_OK)
             goto done;
-        if ((r = upload(b, (void **)&b->d_segB[k], segB[k], nsegB[k] * 4, "sweep segments")) != SG_OK) goto done;
-        for (cls = 0; cls < SG_SWEEP_CLASSES; cls++) {
-            sg_sweep_tables *t = &b->sweepB[k][cls];
-            const int64_t hi = cls + 1 < SG_SWEEP_CLASSES ? first[cls + 1] : nchB[k];
-            t->chains = b->d_chB[k] + first[cls];
-            t->seg = b->d_segB[k];
-            t->nchains = hi - first[cls];
-            t->cap32 = t->cap64 = 0;
-            t->lmax_max = 0;
-            for (i = first[cls]; i < hi; i++) {
-                const int64_t e32 = chain_elems(&chB[k][i], 4), e64 = chain_elems(&chB[k][i], 8);
-                if (e32 > t->cap32) t->cap32 = e32;
-                if (e64 > t->cap64) t->cap64 = e64;
-                if (chB[k][i].lmax > t->lmax_max) t->lmax_max = chB[k][i].lmax;
+        for (q = 0; q < ngr; q++) {
+            int64_t i, first[SG_SWEEP_CLASSES + 1];
+            int cls;
+            const int64_t lo = gfirst[q][k], hi_q = gfirst[q + 1][k];
+            /* classes are contiguous (sorted by size): count, then prefix sums */
+            for (cls = 0; cls <= SG_SWEEP_CLASSES; cls++) first[cls] = lo;
+            for (i = lo; i < hi_q; i++) {
+                const int64_t e32 = chain_elems(&chB[k][i], 4);
+                first[1 + (e32 > 256 * 12 ? 0 : (e32 > 128 * 12 ? 1 : 2))]++;
+            }
+            for (cls = 1; cls <= SG_SWEEP_CLASSES; cls++) first[cls] += first[cls - 1] - lo;
+            for (cls = 0; cls < SG_SWEEP_CLASSES; cls++) {
+                sg_sweep_tables *t = &b->sweepG[((int64_t)q * SG_MAX_DIMS + k) * SG_SWEEP_CLASSES + cls];
+                const int64_t hi = cls + 1 < SG_SWEEP_CLASSES ? first[cls + 1] : hi_q;
+                t->chains = b->d_chB[k] + first[cls];
+                t->seg = b->d_segB[k];
+                t->nchains = hi - first[cls];
+                t->cap32 = t->cap64 = 0;
+                t->lmax_max = 0;
+                for (i = first[cls]; i < hi; i++) {
+                    const int64_t e32 = chain_elems(&chB[k][i], 4), e64 = chain_elems(&chB[k][i], 8);
+                    if (e32 > t->cap32) t->cap32 = e32;
+                    if (e64 > t->cap64) t->cap64 = e64;
+                    if (chB[k][i].lmax > t->lmax_max) t->lmax_max = chB[k][i].lmax;
+                }
             }
         }
     }
@@ -428,6 +472,7 @@ static int materialize(sg_batch *b)
     b->nrepack = nrp;
     r = upload(b, (void **)&b->d_repack, rp, nrp * (int64_t)sizeof(sg_repack), "batch repack table");
 done:
+    free(gfirst);
     free(order);
     free(sg);
     free(sch);
@@ -547,68 +592,112 @@ SG_API int sg_batch_sample_function(sg_batch *b, int fn, const double *params, i
 }
 
 /* The hierarchization launches (also what the graph captures). */
+static const sg_sweep_tables *sweep_table(const sg_batch *b, int q, int k, int c)
+{
+    return &b->sweepG[((int64_t)q * SG_MAX_DIMS + k) * SG_SWEEP_CLASSES + c];
+}
+
+/* One chain-size class of one sweep on stream cs.  Kernel: 2 gather; 3 (or
+ * 0 for the shortest chains) one warp per chain; otherwise the staged chain
+ * kernel where it fits. */
+static int sweep_class(sg_batch *b, const sg_sweep_tables *t, int c, int fp64, cudaStream_t cs)
+{
+    int e;
+    const int kern = b->hier_kernel[c] ? b->hier_kernel[c] : (c == SG_SWEEP_CLASSES - 1 ? 3 : 1);
+    const int64_t cap = fp64 ? t->cap64 : t->cap32;
+    const int eb = fp64 ? 8 : 4;
+    if (kern == 3 && sgk_small_smem_bytes(cap, eb) >= 0)
+        e = fp64 ? sgk_sweep_small_f64(b->d_work, t, cs) : sgk_sweep_small_f32(b->d_alpha, t, cs);
+    else if (kern != 2 && sgk_chain_smem_bytes(cap, eb) >= 0)
+        e = fp64 ? sgk_sweep_chains_f64(b->d_work, t, b->d_err, cs) : sgk_sweep_chains_f32(b->d_alpha, t, b->d_err, cs);
+    else
+        e = fp64 ? sgk_sweep_gather_f64(b->d_work, t, cs) : sgk_sweep_gather_f32(b->d_alpha, t, cs);
+    return e == cudaSuccess ? SG_OK : bcuda((cudaError_t)e, "batch sweep");
+}
+
 static int hier_launches(sg_batch *b, cudaStream_t st)
 {
-    int k, c, e;
+    int k, c, q, r;
+    cudaError_t e;
     const int fp64 = b->precision == SG_HIER_FP64;
     if (b->has_sweep_grids) {
-        if (fp64 && (e = sgk_widen(b->d_alpha, b->d_work, b->doff[b->ng], st)) != cudaSuccess)
-            return bcuda((cudaError_t)e, "widen");
-        for (k = 0; k < SG_MAX_DIMS; k++) {
-            /* the size classes of sweep k are independent: fork them onto
-             * their own streams and join before sweep k+1 */
-            int any = 0;
-            for (c = 0; c < SG_SWEEP_CLASSES; c++) any |= b->sweepB[k][c].nchains > 0;
-            if (!any) continue;
+        if (fp64 && (e = (cudaError_t)sgk_widen(b->d_alpha, b->d_work, b->doff[b->ng], st)) != cudaSuccess)
+            return bcuda(e, "widen");
+        if (b->ngroups == 1) {
+            for (k = 0; k < SG_MAX_DIMS; k++) {
+                /* the size classes of sweep k are independent: fork them
+                 * onto their own streams and join before sweep k+1 */
+                int any = 0;
+                for (c = 0; c < SG_SWEEP_CLASSES; c++) any |= sweep_table(b, 0, k, c)->nchains > 0;
+                if (!any) continue;
+                BCU(cudaEventRecord(b->ev_fork, st), "cudaEventRecord");
+                for (c = 0; c < SG_SWEEP_CLASSES; c++) {
+                    const sg_sweep_tables *t = sweep_table(b, 0, k, c);
+                    cudaStream_t cs = b->dst[1 + c];
+                    if (!t->nchains) continue;
+                    BCU(cudaStreamWaitEvent(cs, b->ev_fork, 0), "cudaStreamWaitEvent");
+                    if ((r = sweep_class(b, t, c, fp64, cs)) != SG_OK) return r;
+                    BCU(cudaEventRecord(b->ev_d[1 + c], cs), "cudaEventRecord");
+                    BCU(cudaStreamWaitEvent(st, b->ev_d[1 + c], 0), "cudaStreamWaitEvent");
+                }
+            }
+        } else {
+            /* groups round-robin over SG_SWEEP_STREAMS streams; on its
+             * stream a group runs sweep 0..d-1, class after class, so its
+             * values stay in L2 from one sweep to the next while the other
+             * streams' groups fill the GPU */
+            const int ns = b->ngroups < SG_SWEEP_STREAMS ? b->ngroups : SG_SWEEP_STREAMS;
             BCU(cudaEventRecord(b->ev_fork, st), "cudaEventRecord");
-            for (c = 0; c < SG_SWEEP_CLASSES; c++) {
-                const sg_sweep_tables *t = &b->sweepB[k][c];
-                cudaStream_t cs = b->dst[1 + c];
-                if (!t->nchains) continue;
-                BCU(cudaStreamWaitEvent(cs, b->ev_fork, 0), "cudaStreamWaitEvent");
-                /* kernel: 2 gather; 3 (or 0 for the shortest chains) one warp
-                 * per chain; otherwise the staged chain kernel where it fits */
-                const int kern = b->hier_kernel[c] ? b->hier_kernel[c] : (c == SG_SWEEP_CLASSES - 1 ? 3 : 1);
-                const int64_t cap = fp64 ? t->cap64 : t->cap32;
-                const int eb = fp64 ? 8 : 4;
-                if (kern == 3 && sgk_small_smem_bytes(cap, eb) >= 0)
-                    e = fp64 ? sgk_sweep_small_f64(b->d_work, t, cs) : sgk_sweep_small_f32(b->d_alpha, t, cs);
-                else if (kern != 2 && sgk_chain_smem_bytes(cap, eb) >= 0)
-                    e = fp64 ? sgk_sweep_chains_f64(b->d_work, t, b->d_err, cs)
-                             : sgk_sweep_chains_f32(b->d_alpha, t, b->d_err, cs);
-                else
-                    e = fp64 ? sgk_sweep_gather_f64(b->d_work, t, cs) : sgk_sweep_gather_f32(b->d_alpha, t, cs);
-                if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch sweep");
-                BCU(cudaEventRecord(b->ev_d[1 + c], cs), "cudaEventRecord");
-                BCU(cudaStreamWaitEvent(st, b->ev_d[1 + c], 0), "cudaStreamWaitEvent");
+            for (q = 0; q < ns; q++) BCU(cudaStreamWaitEvent(b->dst[1 + q], b->ev_fork, 0), "cudaStreamWaitEvent");
+            for (q = 0; q < b->ngroups; q++) {
+                cudaStream_t cs = b->dst[1 + q % ns];
+                for (k = 0; k < SG_MAX_DIMS; k++)
+                    for (c = 0; c < SG_SWEEP_CLASSES; c++) {
+                        const sg_sweep_tables *t = sweep_table(b, q, k, c);
+                        if (t->nchains && (r = sweep_class(b, t, c, fp64, cs)) != SG_OK) return r;
+                    }
+            }
+            for (q = 0; q < ns; q++) {
+                BCU(cudaEventRecord(b->ev_d[1 + q], b->dst[1 + q]), "cudaEventRecord");
+                BCU(cudaStreamWaitEvent(st, b->ev_d[1 + q], 0), "cudaStreamWaitEvent");
             }
         }
-        if (fp64 && (e = sgk_narrow(b->d_work, b->d_alpha, b->doff[b->ng], st)) != cudaSuccess)
-            return bcuda((cudaError_t)e, "narrow");
+        if (fp64 && (e = (cudaError_t)sgk_narrow(b->d_work, b->d_alpha, b->doff[b->ng], st)) != cudaSuccess)
+            return bcuda(e, "narrow");
     }
     /* after the sweeps: their FP64 round trip rewrites the whole buffer with
      * the (unchanged) nodal values of the shared-memory grids */
     for (c = 0; c < SG_BATCH_CLASSES; c++) {
         if (!b->cls_count[c]) continue;
-        e = sgk_hier_smem_grids(b->d_alpha, b->d_smem_grids + b->cls_first[c], b->cls_count[c], b->d_smem_chains,
-                                b->d_smem_seg, b->cls_max_npad[c], fp64, st);
-        if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch shared-memory hierarchization");
+        e = (cudaError_t)sgk_hier_smem_grids(b->d_alpha, b->d_smem_grids + b->cls_first[c], b->cls_count[c],
+                                             b->d_smem_chains, b->d_smem_seg, b->cls_max_npad[c], fp64, st);
+        if (e != cudaSuccess) return bcuda(e, "batch shared-memory hierarchization");
     }
     return SG_OK;
 }
 
-static int run_graph(cudaGraphExec_t *exec, int (*body)(sg_batch *, cudaStream_t), sg_batch *b, cudaStream_t st)
+/* Replays *exec, capturing body into it first.  The library's launch
+ * counter counts kernels as they launch, so a replay adds the kernels the
+ * capture recorded (*kernels). */
+static int run_graph(cudaGraphExec_t *exec, int64_t *kernels, int (*body)(sg_batch *, cudaStream_t), sg_batch *b,
+                     cudaStream_t st)
 {
     cudaGraph_t graph = NULL;
     cudaError_t e;
     int r;
+    int64_t before;
     if (*exec) {
         BCU(cudaGraphLaunch(*exec, st), "cudaGraphLaunch");
+        sgk_count((int)*kernels);
         return SG_OK;
     }
     if (st == 0) return body(b, st); /* the legacy stream cannot be captured */
     BCU(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    before = sgk_launches();
     r = body(b, st);
+    /* captured kernels do not run yet: counted at each replay instead */
+    *kernels = sgk_launches() - before;
+    sgk_count((int)-*kernels);
     e = cudaStreamEndCapture(st, &graph);
     if (r != SG_OK) {
         if (graph) cudaGraphDestroy(graph);
@@ -622,6 +711,7 @@ static int run_graph(cudaGraphExec_t *exec, int (*body)(sg_batch *, cudaStream_t
         return bcuda(e, "cudaGraphInstantiate");
     }
     BCU(cudaGraphLaunch(*exec, st), "cudaGraphLaunch");
+    sgk_count((int)*kernels);
     return SG_OK;
 }
 
@@ -635,7 +725,7 @@ SG_API int sg_batch_hierarchize_async(sg_batch *b, void *stream)
     if (b->precision == SG_HIER_FP64 && b->has_sweep_grids && !b->d_work)
         r = balloc(b, (void **)&b->d_work, b->doff[b->ng] * 8, "batch FP64 working values");
     if (r == SG_OK) r = make_fork_streams(b);
-    if (r == SG_OK) r = b->use_graph ? run_graph(&b->hier_graph, hier_launches, b, st) : hier_launches(b, st);
+    if (r == SG_OK) r = b->use_graph ? run_graph(&b->hier_graph, &b->hier_graph_kernels, hier_launches, b, st) : hier_launches(b, st);
     b->eval_dirty = 1;
     leave(b, prev);
     return r;
@@ -892,7 +982,7 @@ SG_API int sg_batch_evaluate_device(sg_batch *b, const int64_t *point_offsets, c
     if (point_offsets[b->ng] >= ((int64_t)1 << 31)) return bfail(SG_ERR_RANGE, "sg_batch_evaluate: too many points");
     if ((r = enter(b, &prev)) != SG_OK) return r;
     if ((r = make_fork_streams(b)) == SG_OK && (r = plan_eval(b, point_offsets, coords, out)) == SG_OK)
-        r = b->use_graph ? run_graph(&b->eval_graph, eval_launches, b, st) : eval_launches(b, st);
+        r = b->use_graph ? run_graph(&b->eval_graph, &b->eval_graph_kernels, eval_launches, b, st) : eval_launches(b, st);
     if (r == SG_OK) b->eval_dirty = 0;
     leave(b, prev);
     return r;
@@ -904,7 +994,7 @@ SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const fl
     cudaStream_t st = (cudaStream_t)stream;
     cudaEvent_t e0 = NULL, e1 = NULL;
     double t[2][SG_MAX_DIMS + 1];
-    int prev, r, pi, k, rep;
+    int prev, r, pi, k, q, rep;
     float el;
     if (!b || !point_offsets || point_offsets[0] != 0) return bfail(SG_ERR_ARG, "sg_batch_autotune: bad argument");
     if (!b->has_values || b->dev < 0) return bfail(SG_ERR_STATE, "sg_batch_autotune: no values have been set");
@@ -967,7 +1057,8 @@ SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const fl
         for (c = 0; c < SG_SWEEP_CLASSES && r == SG_OK; c++) {
             double best = -1.0;
             int best_k = 0, any = 0;
-            for (k = 0; k < SG_MAX_DIMS; k++) any |= b->sweepB[k][c].nchains > 0;
+            for (q = 0; q < b->ngroups; q++)
+                for (k = 0; k < SG_MAX_DIMS; k++) any |= sweep_table(b, q, k, c)->nchains > 0;
             if (!any) continue;
             for (kern = 1; kern <= 3 && r == SG_OK; kern += 2) {
                 b->hier_kernel[c] = kern;
@@ -1043,6 +1134,13 @@ SG_API int sg_batch_set_option(sg_batch *b, int option, int64_t value)
         }
         return SG_OK;
     }
+    case SG_OPT_SWEEP_GROUP:
+        /* the sweep tables are built by the first device call */
+        if (value < 0 || value >= ((int64_t)1 << 32)) return bfail(SG_ERR_ARG, "SG_OPT_SWEEP_GROUP is 0 .. 2^32-1");
+        if (b->dev >= 0 && value != b->sweep_group)
+            return bfail(SG_ERR_STATE, "SG_OPT_SWEEP_GROUP must be set before the batch's first device call");
+        b->sweep_group = value;
+        return SG_OK;
     default:
         return bfail(SG_ERR_ARG, "option %d does not apply to batches", option);
     }

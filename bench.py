@@ -424,7 +424,10 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     nflt = int(np.sum(counts * dims))
     X = torch.from_numpy(inputs.uniform01(SEED + 100 + rank, nflt)).to(dev)
     out = torch.empty(int(po[-1]), dtype=torch.float32, device=dev)
-    stream = torch.cuda.current_stream()
+    # a stream of its own: the legacy default stream cannot be captured, and
+    # on this one the batch captures its launches once and replays the graphs
+    stream = torch.cuda.Stream(device=dev)
+    stream.wait_stream(torch.cuda.current_stream())
     b.set_values_device(vals, stream)
     b.hierarchize_async(stream)
     tuned = b.autotune(po, X, out, stream)  # points per thread per dimension
@@ -493,6 +496,9 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     plain_value = plain_pts / (plain_ms / 1e3)
     if rank != 0:
         return
+    err = None
+    if world == 1 and not args.no_cpu_baseline:
+        err = batch_error_vs_fp64(b, vals.cpu().numpy(), dims, levels, out.cpu().numpy(), xs, po, coff)
     hier_bytes = 8.0 * float(np.sum(np.array(npts) * dims))
     line = {
         "metric": "evals/s (batched grids)", "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
@@ -509,7 +515,33 @@ def run_batched(args, rank: int, world: int, local_rank: int):
         "speedup_vs_plain": value / plain_value, "autotuned_ppt_by_d": tuned_ppt,
         "gpu_launches": int(launches), "clocks": clk.summary(),
     }
+    if err is not None:
+        line["err_vs_fp64"] = err
     print(json.dumps(line), flush=True)
+
+
+def batch_error_vs_fp64(b, nodal: np.ndarray, dims, levels, out: np.ndarray, xs: np.ndarray, po, coff,
+                        per_d: int = 2, npts: int = 64):
+    """Error of the batched results against the FP64 oracle (checker only):
+    for `per_d` grids of every dimension, FP64 hierarchization of the grid's
+    nodal values and FP64 evaluation at `npts` of its query points."""
+    from oracle.oracle import Oracle
+    worst_abs, worst_rel, checked = 0.0, 0.0, 0
+    for d in sorted(set(int(x) for x in dims)):
+        for g in [int(i) for i in np.flatnonzero(dims == d)[:per_d]]:
+            o = Oracle(d, int(levels[g]), None)
+            s64 = o.hierarchize_f64(b.grid_values(nodal, g).astype(np.float64))
+            m = int(po[g + 1] - po[g])
+            idx = np.linspace(0, m - 1, min(npts, m)).astype(np.int64)
+            Xg = xs[coff[g]:coff[g + 1]].reshape(m, d)
+            u64 = o.evaluate_f64(s64, Xg[idx])
+            e = np.abs(out[po[g]:po[g + 1]][idx].astype(np.float64) - u64)
+            scale = max(float(np.max(np.abs(u64))), 1e-30)
+            worst_abs = max(worst_abs, float(e.max()))
+            worst_rel = max(worst_rel, float(e.max()) / scale)
+            checked += 1
+    return {"grids": checked, "points_per_grid": npts, "max_abs": worst_abs, "max_norm_rel": worst_rel,
+            "note": "FP32 batched results vs FP64 hierarchize + evaluate of the same nodal values"}
 
 
 def run_served(args, rank: int, world: int, local_rank: int):

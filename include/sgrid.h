@@ -65,6 +65,10 @@ extern "C" {
                                 /* 3 = one warp per chain (batches only)            */
 #define SG_OPT_PROFILE 6        /* 1: record CUDA events around each phase            */
 #define SG_OPT_USE_GRAPH 7      /* batches: 1 (default) capture launches in a CUDA graph */
+#define SG_OPT_SWEEP_GROUP 8    /* batches: values per sweep group (default 2^22): all   */
+                                /* sweeps of a group run back to back so it stays in  */
+                                /* L2; 0 = every sweep over the whole batch.  Set it  */
+                                /* before the batch's first device call.             */
 
 /* Phases reported by sg_timings (milliseconds of the most recent call). */
 #define SG_PHASE_HIERARCHIZE 0  /* all sweeps of the last hierarchization    */
@@ -231,7 +235,8 @@ int sg_batch_evaluate_device(sg_batch *batch, const int64_t *point_offsets, cons
                              float *out, void *stream);
 int sg_batch_sync(sg_batch *batch, void *stream);
 /* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH, SG_OPT_HIER_KERNEL (sweeps),
- * SG_OPT_EVAL_SORT (1, default: each grid's points spatially ordered on the GPU) */
+ * SG_OPT_EVAL_SORT (1, default: each grid's points spatially ordered on the GPU),
+ * SG_OPT_SWEEP_GROUP (before the first device call; SG_ERR_STATE after it) */
 int sg_batch_set_option(sg_batch *batch, int option, int64_t value);
 /* Autotuner for batches (no reference counterpart): times each
  * dimension's evaluation launch over the caller's points at 1 and at 2

@@ -35,7 +35,7 @@ def test_header_constants_match_bindings():
     text = open(_lib.HEADER).read()
     for name in ["SG_MAX_DIMS", "SG_MAX_LEVELS", "SG_OK", "SG_HIER_FP64", "SG_OPT_HIER_PRECISION",
                  "SG_OPT_EVAL_SORT", "SG_OPT_EVAL_PPT", "SG_OPT_HIER_KERNEL", "SG_OPT_PROFILE",
-                 "SG_FN_GAUSS", "SG_FN_QUAD", "SG_NUM_PHASES"]:
+                 "SG_OPT_USE_GRAPH", "SG_OPT_SWEEP_GROUP", "SG_FN_GAUSS", "SG_FN_QUAD", "SG_NUM_PHASES"]:
         import re
         m = re.search(rf"#define {name} \(?(-?\d+)\)?", text)
         assert m, name
@@ -119,6 +119,17 @@ def test_options_validate():
                      (sg.SG_OPT_HIER_KERNEL, -1), (99, 0)]:
         with pytest.raises(sg.SgError):
             grid.set_option(opt, bad)
+
+
+def test_batch_sweep_group_option_validates():
+    # host-only: the sweep tables are built by the batch's first device call
+    b = sg.Batch([3, 10], [4, 6])
+    for ok in (0, 1, 1 << 22):
+        b.set_option(_lib.SG_OPT_SWEEP_GROUP, ok)
+    for bad in (-1, 1 << 32):
+        with pytest.raises(sg.SgError):
+            b.set_option(_lib.SG_OPT_SWEEP_GROUP, bad)
+    b.close()
 
 
 def test_calls_before_values_are_state_errors():

@@ -24,11 +24,16 @@ def _batch(shapes):
 
 
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
-@pytest.mark.parametrize("graph,kernel", [(1, 0), (0, 0), (1, 1), (1, 3)])
-def test_batch_hierarchize_matches_single_grids(cuda, precision, graph, kernel):
+@pytest.mark.parametrize("graph,kernel,group", [(1, 0, None), (0, 0, None), (1, 1, None), (1, 3, None),
+                                                (1, 0, 0), (1, 0, 1), (0, 3, 1 << 15)])
+def test_batch_hierarchize_matches_single_grids(cuda, precision, graph, kernel, group):
     # kernel 0: auto (short chains one warp per chain), 1: staged chains
-    # everywhere, 3: one warp per chain wherever the chains fit
+    # everywhere, 3: one warp per chain wherever the chains fit; group: values
+    # per sweep group (None: default, 0: every sweep over the whole batch,
+    # 1: one group per grid, run on several streams)
     b = _batch(MIXED)
+    if group is not None:
+        b.set_option(_lib.SG_OPT_SWEEP_GROUP, group)
     b.set_option(_lib.SG_OPT_USE_GRAPH, graph)
     b.set_option(_lib.SG_OPT_HIER_KERNEL, kernel)
     b.set_option(_lib.SG_OPT_HIER_PRECISION, _lib.SG_HIER_FP64 if precision == "fp64" else _lib.SG_HIER_FP32)
