@@ -64,6 +64,9 @@ def parse():
                     help="single: the d=10 n=10 grid (default); adaptive: the refined d=6 grid; batched: many "
                          "grids of mixed d and n; served: Poisson request stream against resident grids")
     ap.add_argument("--grids", type=int, default=4096, help="batched: number of grids")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="batched: launch kernels directly instead of replaying CUDA graphs (for profilers that "
+                         "cannot follow stream capture)")
     ap.add_argument("--rates", default="1000,2000,4000,8000,16000", help="served: arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=3000, help="served: requests per rate")
     ap.add_argument("--cap-gb", type=float, default=60.0, help="served: resident-grid byte cap")
@@ -410,13 +413,14 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     import torch
     from adaptive_sparse_grid_bench_b200 import Batch, Grid, inputs
     from adaptive_sparse_grid_bench_b200._lib import (SG_FN_QUAD, SG_HIER_FP32, SG_HIER_FP64, SG_OPT_HIER_PRECISION,
-                                                      kernel_launches)
+                                                      SG_OPT_USE_GRAPH, kernel_launches)
     from adaptive_sparse_grid_bench_b200.sharding import max_over_ranks
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     dims, levels, coef, counts = inputs.batch_workload(3 + rank, args.grids)
     b = Batch(dims, levels)
     b.set_option(SG_OPT_HIER_PRECISION, SG_HIER_FP64 if args.precision == "fp64" else SG_HIER_FP32)
+    b.set_option(SG_OPT_USE_GRAPH, 0 if args.no_graph else 1)
     b.sample_function(SG_FN_QUAD, coef)
     vals = torch.empty(b.num_values, dtype=torch.float32, device=dev)
     b.get_values_device(vals)
@@ -506,7 +510,8 @@ def run_batched(args, rank: int, world: int, local_rank: int):
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64)",
         "config": {"workload": f"{len(dims)} grids, d in 2..12, n in 3..9, <= 2e6 points each, f = prod(a+bx+cx^2),"
                                f" 256..65536 log-uniform points per grid", "grids": len(dims),
-                   "grid_points": int(sum(npts)), "query_points": total_pts, "hier_precision": args.precision},
+                   "grid_points": int(sum(npts)), "query_points": total_pts, "hier_precision": args.precision,
+                   "cuda_graphs": not args.no_graph},
         "hierarchize": {"ms": statistics.mean(th), "GB/s_8dN": hier_bytes / (statistics.mean(th) / 1e3) / 1e9,
                         "grids_per_s": len(dims) / (statistics.mean(th) / 1e3)},
         "evaluate": {"ms": statistics.mean(te), "evals_per_s": total_pts / (statistics.mean(te) / 1e3)},
