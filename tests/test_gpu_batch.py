@@ -140,3 +140,31 @@ def test_batch_autotune_keeps_results(cuda):
     b.set_values(vals)
     b.hierarchize()
     assert np.array_equal(b.get_values().view(np.uint32), surplus.view(np.uint32))
+
+
+def test_batch_graph_replays_on_a_stream_are_counted(cuda):
+    """On a non-default stream the batch captures its launches once and
+    replays the graph; every replay adds the captured kernels to the
+    library's launch counter, and gives the same surpluses as direct
+    launches."""
+    import torch
+    vals = inputs.uniform01(81, _batch(MIXED).num_values) * 2 - 1
+    direct = _batch(MIXED)
+    direct.set_option(_lib.SG_OPT_USE_GRAPH, 0)
+    direct.set_values(vals)
+    st = torch.cuda.Stream(device=cuda)
+    l0 = _lib.kernel_launches()
+    direct.hierarchize_async(st)
+    direct.sync(st)
+    per_run = _lib.kernel_launches() - l0
+    assert per_run > 0
+    want = direct.get_values()
+    g = _batch(MIXED)
+    g.set_values(vals)
+    for rep in range(3):  # capture + launch, then two replays
+        g.set_values(vals)
+        l0 = _lib.kernel_launches()
+        g.hierarchize_async(st)
+        g.sync(st)
+        assert _lib.kernel_launches() - l0 == per_run, f"run {rep}"
+        assert np.array_equal(g.get_values().view(np.uint32), want.view(np.uint32))
