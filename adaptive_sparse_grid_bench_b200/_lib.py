@@ -32,6 +32,7 @@ SG_OPT_HIER_KERNEL = 5
 SG_OPT_PROFILE = 6
 SG_OPT_USE_GRAPH = 7
 SG_OPT_SWEEP_GROUP = 8
+SG_OPT_TEST_WAIT = 9
 SG_NUM_PHASES = 3
 
 SG_FN_REFERENCE = 0

@@ -30,7 +30,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kMaxStages = 2;
-constexpr long long kWaitCycles = 4000000000LL; /* ~2 s at 1.9 GHz */
+constexpr long long kWaitCycles = 4000000000LL; /* ~2 s at 1.9 GHz: the default wait limit */
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -63,13 +63,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-/* Bounded wait: gives up after kWaitCycles and reports false. */
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+/* Bounded wait: gives up after `limit` clock cycles and reports false. */
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, long long limit)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const long long t0 = clock64();
     while (!mbar_try_wait(bar, parity))
-        if (clock64() - t0 > kWaitCycles) return false;
+        if (clock64() - t0 > limit) return false;
     return true;
 }
 
@@ -225,7 +225,8 @@ template <typename T, int NT>
 __global__ void __launch_bounds__(NT) k_sweep_chains(T *__restrict__ a,
                                                           const sg_chain *__restrict__ chains,
                                                           const uint32_t *__restrict__ seg,
-                                                          int nch, int cap, int nst, int *__restrict__ err)
+                                                          int nch, int cap, int nst, int *__restrict__ err,
+                                                          long long wait_limit, int stall)
 {
     constexpr int A = 16 / sizeof(T); /* elements per 16 bytes */
     using V = typename Vec<T>::type;
@@ -238,7 +239,10 @@ __global__ void __launch_bounds__(NT) k_sweep_chains(T *__restrict__ a,
     const int tid = threadIdx.x;
 
     /* chain c goes to stage b; the stage's barrier completes when all its
-     * bulk copies have landed */
+     * bulk copies have landed.  With `stall` (the wait-timeout test), the
+     * first chain of every CTA announces its bytes (at least 16) but issues
+     * no copy, so its wait can only run out: no copy is ever in flight
+     * towards that stage. */
     auto issue = [&](int c, int b) {
         const sg_chain ch = chains[c];
         T *dst = stage0 + (size_t)b * cap;
@@ -248,6 +252,10 @@ __global__ void __launch_bounds__(NT) k_sweep_chains(T *__restrict__ a,
             if (sz >= 16) bytes += sz;
         }
         fence_proxy_async();
+        if (stall && c == (int)blockIdx.x) {
+            mbar_arrive_expect_tx(&bar[b], bytes < 16 ? 16u : bytes);
+            return;
+        }
         mbar_arrive_expect_tx(&bar[b], bytes);
         for (int j = 0; j <= ch.lmax; ++j) {
             const uint32_t sz = (uint32_t)sizeof(T) << (ch.sigma + j);
@@ -272,7 +280,7 @@ __global__ void __launch_bounds__(NT) k_sweep_chains(T *__restrict__ a,
         const sg_chain ch = chains[c];
         const int sigma = ch.sigma, lo = ch.lo, lmax = ch.lmax;
         T *buf = stage0 + (size_t)b * cap;
-        if (!mbar_wait(&bar[b], parity)) {
+        if (!mbar_wait(&bar[b], parity, wait_limit)) {
             atomicExch(err, 1);
             s_abort = 1;
         }
@@ -319,7 +327,7 @@ __global__ void __launch_bounds__(NT) k_sweep_chains(T *__restrict__ a,
         /* let the copies still in flight land before the CTA exits: every
          * stage issued for iterations abort_it .. abort_it+nst-1 (bounded) */
         for (int q = abort_it; q < abort_it + nst; ++q)
-            if (blockIdx.x + q * G < nch) (void)mbar_wait(&bar[q % nst], (q / nst) & 1);
+            if (blockIdx.x + q * G < nch) (void)mbar_wait(&bar[q % nst], (q / nst) & 1, wait_limit);
     }
 }
 
@@ -389,7 +397,8 @@ int g_num_sms = 0;
 long long g_launches = 0;
 
 template <typename T, int NT>
-int launch_chains_nt(T *a, const sg_sweep_tables *t, int64_t cap, int *err, void *stream)
+int launch_chains_nt(T *a, const sg_sweep_tables *t, int64_t cap, int *err, long long wait_limit, int stall,
+                     void *stream)
 {
     const int64_t stage_bytes = (cap * (int64_t)sizeof(T) + 127) / 128 * 128;
     /* as many stages (2..kMaxStages) as fit in 96 KB */
@@ -407,7 +416,7 @@ int launch_chains_nt(T *a, const sg_sweep_tables *t, int64_t cap, int *err, void
     int64_t grid = (int64_t)sgk_num_sms() * per_sm;
     if (grid > t->nchains) grid = t->nchains;
     k_sweep_chains<T, NT><<<(unsigned)grid, NT, (size_t)smem, (cudaStream_t)stream>>>(
-        a, t->chains, t->seg, (int)t->nchains, capi, nst, err);
+        a, t->chains, t->seg, (int)t->nchains, capi, nst, err, wait_limit, stall);
     sgk_count(1);
     return cudaGetLastError();
 }
@@ -415,14 +424,15 @@ int launch_chains_nt(T *a, const sg_sweep_tables *t, int64_t cap, int *err, void
 /* CTA size follows the chain size: up to 12 elements (three 16-byte groups)
  * per thread, between 128 and 512 threads. */
 template <typename T>
-int launch_chains(T *a, const sg_sweep_tables *t, int *err, void *stream)
+int launch_chains(T *a, const sg_sweep_tables *t, int *err, void *stream, long long wait_limit = kWaitCycles,
+                  int stall = 0)
 {
     if (t->nchains == 0) return cudaSuccess;
     const int64_t cap = sizeof(T) == 4 ? t->cap32 : t->cap64;
     if (sgk_chain_smem_bytes(cap, (int)sizeof(T)) < 0) return cudaErrorInvalidValue;
-    if (cap <= 128 * 12) return launch_chains_nt<T, 128>(a, t, cap, err, stream);
-    if (cap <= 256 * 12) return launch_chains_nt<T, 256>(a, t, cap, err, stream);
-    return launch_chains_nt<T, 512>(a, t, cap, err, stream);
+    if (cap <= 128 * 12) return launch_chains_nt<T, 128>(a, t, cap, err, wait_limit, stall, stream);
+    if (cap <= 256 * 12) return launch_chains_nt<T, 256>(a, t, cap, err, wait_limit, stall, stream);
+    return launch_chains_nt<T, 512>(a, t, cap, err, wait_limit, stall, stream);
 }
 
 /* Small chains (the many short chains of batched grids): one warp per
@@ -565,6 +575,11 @@ int sgk_sweep_chains_f32(float *a, const sg_sweep_tables *t, int *err, void *str
 int sgk_sweep_chains_f64(double *a, const sg_sweep_tables *t, int *err, void *stream)
 {
     return launch_chains<double>(a, t, err, stream);
+}
+int sgk_sweep_chains_stall_f32(float *a, const sg_sweep_tables *t, int *err, long long wait_limit, void *stream)
+{
+    if (wait_limit < 1 || wait_limit > kWaitCycles) return cudaErrorInvalidValue;
+    return launch_chains<float>(a, t, err, stream, wait_limit, 1);
 }
 int sgk_sweep_small_f32(float *a, const sg_sweep_tables *t, void *stream)
 {

@@ -11,10 +11,15 @@
  * device array, not a device address: a kernel given it would fault or, where
  * the GPU can reach host memory, use the wrong memory.  The device address is
  * obtained once per device with cudaGetSymbolAddress, with that device
- * current, and cached here.
+ * current, and cached here; the cache entries are atomic, so host threads
+ * may call concurrently.  A cudaDeviceReset ends every device allocation of
+ * this library on that device, the cached address included: handles and
+ * this cache do not survive it.
  */
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <atomic>
 
 #include "sg_kernels.h"
 
@@ -23,7 +28,7 @@ namespace {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SG_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-void *g_scratch_ptr[kMaxDevices];
+std::atomic<void *> g_scratch_ptr[kMaxDevices];
 
 } // namespace
 
@@ -33,13 +38,14 @@ extern "C" int sgk_noalloc_scratch(void **ptr, int64_t *bytes)
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
+    void *p = g_scratch_ptr[dev].load(std::memory_order_acquire);
+    if (!p) {
+        /* two threads may both look it up: they store the same address */
         e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        g_scratch_ptr[dev] = p;
+        g_scratch_ptr[dev].store(p, std::memory_order_release);
     }
-    *ptr = g_scratch_ptr[dev];
+    *ptr = p;
     *bytes = SG_NOALLOC_SCRATCH_BYTES;
     return cudaSuccess;
 }

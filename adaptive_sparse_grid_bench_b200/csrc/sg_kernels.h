@@ -31,6 +31,11 @@ int64_t sgk_chain_smem_bytes(int64_t cap_elems, int elem_bytes);
  * memory with bulk copies.  err: device int, set nonzero on a wait timeout. */
 int sgk_sweep_chains_f32(float *a, const sg_sweep_tables *t, int *err, void *stream);
 int sgk_sweep_chains_f64(double *a, const sg_sweep_tables *t, int *err, void *stream);
+/* The wait-timeout test of sgk_sweep_chains_f32: the first chain of every
+ * CTA announces its copy bytes but issues no copy, so its bounded wait runs
+ * out after wait_limit clock cycles (1 .. the default ~2 s limit); every CTA
+ * sets *err and returns.  The grid's values are left partly swept. */
+int sgk_sweep_chains_stall_f32(float *a, const sg_sweep_tables *t, int *err, long long wait_limit, void *stream);
 /* The same sweep as lmax_max launches, finest level first, gathering the
  * parents from global memory (any chain size). */
 int sgk_sweep_gather_f32(float *a, const sg_sweep_tables *t, void *stream);

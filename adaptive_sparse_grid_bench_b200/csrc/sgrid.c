@@ -479,8 +479,11 @@ static int hierarchize_on(sg_grid *g, cudaStream_t st)
     }
     for (k = 0; k < L->d; k++) {
         const int fits = sgk_chain_smem_bytes(g->sweep[k].cap32, 4) >= 0;
-        e = (kern != 2 && fits) ? sgk_sweep_chains_f32(g->d_alpha, &g->sweep[k], g->d_err, st)
-                                : sgk_sweep_gather_f32(g->d_alpha, &g->sweep[k], st);
+        if (g->opt[SG_OPT_TEST_WAIT] > 0 && fits)
+            e = sgk_sweep_chains_stall_f32(g->d_alpha, &g->sweep[k], g->d_err, g->opt[SG_OPT_TEST_WAIT] << 20, st);
+        else
+            e = (kern != 2 && fits) ? sgk_sweep_chains_f32(g->d_alpha, &g->sweep[k], g->d_err, st)
+                                    : sgk_sweep_gather_f32(g->d_alpha, &g->sweep[k], st);
         if (e != cudaSuccess) return cuda_fail((cudaError_t)e, "FP32 sweep");
     }
     return SG_OK;
@@ -873,6 +876,9 @@ SG_API int sg_set_option(sg_grid *g, int option, int64_t value)
         break;
     case SG_OPT_PROFILE:
         if (value != 0 && value != 1) return fail(SG_ERR_ARG, "SG_OPT_PROFILE is 0 or 1");
+        break;
+    case SG_OPT_TEST_WAIT:
+        if (value < 0 || value > 2048) return fail(SG_ERR_ARG, "SG_OPT_TEST_WAIT is 0 .. 2048");
         break;
     default:
         return fail(SG_ERR_ARG, "unknown option %d", option);

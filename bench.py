@@ -14,11 +14,18 @@ in HBM; `e2e` is the same metric through the C ABI's host-buffer calls
 (sg_set_values / sg_hierarchize / sg_evaluate) with the host<->device copies
 inside the timed region.  Inputs (132 MB grid + 671 MB points per rank) are
 larger than the 126 MB L2, so no flush is needed between steps.
+With --gpus N > 1 and no torchrun environment, the bench starts N local
+ranks itself (torch.distributed.run, NCCL); each rank holds a replica of the
+grid and evaluates its own 2^24 points (weak scaling), and the step time is
+the slowest rank's.
 `--impl reference` times the reference's own C/OpenMP code
 (omp_hierarchize3 + omp_evaluate5, compiled in place into oracle/_ref) on the
-host cores, on a bounded sample of the same workload.  Before timing, the
-library's autotuner picks the evaluation and sweep settings on the bench's
-own buffers (no setting changes a result).
+host cores, on a bounded sample of the same workload, with inputs built by
+the checker side (oracle/) only.  Before timing, the library's autotuner
+picks the evaluation and sweep settings on the bench's own buffers (no
+setting changes a result).  At N=1 the default line also carries compact
+results of the other workloads (`batched`, `served`, `adaptive`), each with
+its error against the FP64 oracle.
 
 Other workloads (`--workload`): `adaptive` (the limits-adaptive d=6 grid
 refined by sg_refine, 2^22 points), `batched` (4096 grids of mixed d and n
@@ -41,11 +48,19 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 D, NLEV, M_EVAL, SEED = 10, 10, 1 << 24, 1
-# DRAM bytes (read + write) of one k_evaluate launch of the default workload
-# (2^24 points), from one ncu capture of this bench; summary and command in
-# profiles/k_evaluate_d10n10_2p24pts_dram.md
-EVAL_TRAFFIC_2P24 = 2.02e9 + 0.553e9
+N_POINTS, N_SUBSPACES = 32_978_945, 92_378
 WORKLOAD = "regular sparse grid d=10 n=10 (N=32,978,945), f=exp(-|x|^2), hierarchize + evaluate 2^24 uniform points"
+EVAL_SRC = os.path.join(ROOT, "adaptive_sparse_grid_bench_b200", "csrc", "eval_impl.cuh")
+# Figures of one k_evaluate launch of the default workload, measured with ncu
+# on the evaluation source whose sha256 starts with `source_sha16`; they are
+# reported only while that source is unchanged (null otherwise).
+#   dram_bytes: dram__bytes_read.sum + dram__bytes_write.sum of one full
+#     2^24-point launch (one-pass metrics, so the full launch was captured);
+#   inst_per_pair: smsp__inst_executed.sum x 32 / (points x subspaces) of a
+#     262,144-point launch of the same grid.
+EVAL_CAPTURE = {"source_sha16": "1330356f2d1d44e3", "captured": "2026-12-04", "dram_bytes": 2.02e9 + 0.553e9,
+                "inst_per_pair": 12.9}
+SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
 def parse():
@@ -59,7 +74,10 @@ def parse():
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU work per reference sample")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="single: leave out the compact batched/served/adaptive results of the N=1 line")
+    ap.add_argument("--cpu-seconds", type=float, default=None,
+                    help="CPU work per reference step (default: about 150 s over all steps, 1.5..12 s each)")
     ap.add_argument("--workload", default="single", choices=["single", "adaptive", "batched", "served"],
                     help="single: the d=10 n=10 grid (default); adaptive: the refined d=6 grid; batched: many "
                          "grids of mixed d and n; served: Poisson request stream against resident grids")
@@ -131,7 +149,7 @@ def single_workload():
     from adaptive_sparse_grid_bench_b200._lib import SG_FN_GAUSS
     return {"name": WORKLOAD, "d": D, "n": NLEV, "limits": None, "fn": SG_FN_GAUSS, "params": (),
             "m_eval": M_EVAL, "make_grid": lambda: Grid(D, NLEV),
-            "points": lambda rank, m: inputs.uniform_points(SEED + rank, m, D),
+            "points": lambda rank, m: inputs.uniform_points(rank_seed(SEED, rank), m, D),
             "l2": "inputs larger than L2 (132 MB grid + 671 MB points)", "info": {}}
 
 
@@ -156,8 +174,9 @@ def adaptive_workload(args):
 
     def points(rank, m):
         h = m // 2
-        return np.concatenate([inputs.uniform_points(2 + 100 * rank, h, d),
-                               inputs.gaussian_points(2 + 100 * rank, m - h, d, 0.3, 0.1, start=1 << 40)])
+        seed = rank_seed(2, rank, 100)
+        return np.concatenate([inputs.uniform_points(seed, h, d),
+                               inputs.gaussian_points(seed, m - h, d, 0.3, 0.1, start=1 << 40)])
 
     wl = {"name": "limits-adaptive grid d=6 from n=4, tol 1e-4, level <= 13, f=exp(-50|x-0.3|^2), "
                   "evaluate 2^22 points (half uniform, half N(0.3,0.1) clipped)",
@@ -166,38 +185,88 @@ def adaptive_workload(args):
     return wl
 
 
-def reference_cpu(values: np.ndarray, X: np.ndarray, seconds: float, wl=None):
-    """Times the reference's own CPU path (oracle/_ref) on a bounded sample:
-    omp_hierarchize3 over the whole grid, omp_evaluate5 over as many query
-    points as fit in `seconds` (16K-point chunks: the SSE variant keeps the
-    coordinates in a stack array).  Returns (per-step evals/s, info)."""
-    from oracle.oracle import Reference
+def cpu_step_seconds(args) -> float:
+    """CPU time per reference step: about 150 s over warm-up + timed steps,
+    between 1.5 and 12 s per step."""
+    if args.cpu_seconds is not None:
+        return args.cpu_seconds
+    return min(12.0, max(1.5, 150.0 / max(1, args.steps + args.warmup)))
+
+
+class ReferenceCPU:
+    """The reference's own CPU path (oracle/_ref, compiled in place) on one
+    grid: a step is omp_hierarchize3 over the whole grid (c:1180) plus
+    omp_evaluate5 (c:1708) over a fixed sample of the query points, sized
+    once to `seconds` of CPU work; the step's evals/s is extrapolated
+    linearly from the sample to the workload's point count."""
+
+    def __init__(self, d, n, limits, values, X, m_step, seconds):
+        from oracle.oracle import Reference
+        self.r = Reference(d, n, limits)
+        self.values, self.X, self.m_step = values, X, m_step
+        self.r.set_values(values)
+        t0 = time.perf_counter()
+        self.r.hierarchize(9)
+        t_h = time.perf_counter() - t0
+        probe = min(2048, X.shape[0])
+        t0 = time.perf_counter()
+        self.r.evaluate(X[:probe], 7)
+        t_probe = time.perf_counter() - t0
+        m = int(probe * max(seconds - t_h, 0.5) / max(t_probe, 1e-6))
+        self.m = int(min(X.shape[0], max(probe, (m // 2048) * 2048)))
+        self.cores = int(self.r.lib().ref_max_threads())
+
+    def step(self):
+        """One step; returns (seconds measured, extrapolated evals/s, parts)."""
+        self.r.set_values(self.values)
+        t0 = time.perf_counter()
+        self.r.hierarchize(9)
+        t_h = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        out = self.r.evaluate(self.X[:self.m], 7)
+        t_e = time.perf_counter() - t0
+        full = t_h + t_e * (self.m_step / self.m)
+        return t_h + t_e, self.m_step / full, {"t_hierarchize_s": t_h, "t_eval_sample_s": t_e, "out": out}
+
+    def one_thread(self, npts: int):
+        """The serial variants: hierarchize7 (c:1009) over the whole grid and
+        evaluate5 (c:1558) over `npts` points."""
+        self.r.set_values(self.values)
+        t0 = time.perf_counter()
+        self.r.hierarchize(7)
+        t_h = time.perf_counter() - t0
+        npts = min(npts, self.X.shape[0])
+        t0 = time.perf_counter()
+        self.r.evaluate(self.X[:npts], 5)
+        t_e = time.perf_counter() - t0
+        return t_h, t_e, npts
+
+
+def reference_cpu(values: np.ndarray, X: np.ndarray, seconds: float, wl=None, one_thread_points: int = 0):
+    """cpu_baseline of the b200 line: one ReferenceCPU step (after one
+    warm-up step) and, optionally, the 1-thread variants."""
     wl = wl or single_workload()
-    M_STEP = wl["m_eval"]
-    r = Reference(wl["d"], wl["n"], wl["limits"])
-    r.set_values(values)
-    t0 = time.perf_counter()
-    r.hierarchize(9)
-    t_h = time.perf_counter() - t0
-    probe = 2048
-    t0 = time.perf_counter()
-    r.evaluate(X[:probe], 7)
-    t_probe = time.perf_counter() - t0
-    m = int(min(X.shape[0], max(probe, probe * max(seconds - t_h, 1.0) / max(t_probe, 1e-6))))
-    m = max(probe, (m // 2048) * 2048)
-    t0 = time.perf_counter()
-    out = r.evaluate(X[:m], 7)
-    t_e = time.perf_counter() - t0
-    per_step = t_h + t_e * (M_STEP / m)
-    info = {"cores": int(r.lib().ref_max_threads()), "t_hierarchize_s": t_h, "t_eval_sample_s": t_e,
-            "sample_points": m, "ref_out": out, "surplus": r.values()}
-    return M_STEP / per_step, info
+    rc = ReferenceCPU(wl["d"], wl["n"], wl["limits"], values, X, wl["m_eval"], seconds)
+    rc.step()
+    _, rate, parts = rc.step()
+    hier_bytes = 8.0 * wl["d"] * values.size
+    info = {"cores": rc.cores, "sample_points": rc.m, "ref_out": parts["out"], "surplus": rc.r.values(),
+            "hierarchize_gbs": {"omp_hierarchize3": hier_bytes / parts["t_hierarchize_s"] / 1e9,
+                                "threads": rc.cores, "bytes": "8*d*N"}}
+    if one_thread_points:
+        t_h, t_e, npts = rc.one_thread(one_thread_points)
+        info["one_thread"] = {"evals_per_s": wl["m_eval"] / (t_h + t_e * wl["m_eval"] / npts),
+                              "hierarchize7_gbs": hier_bytes / t_h / 1e9, "evaluate5_evals_per_s": npts / t_e,
+                              "sample_points": npts}
+    return rate, info
 
 
-def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsample: int = 192, ref_out=None,
+def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsample: int = 1024, ref_out=None,
                   wl=None):
-    """Max/relative error of the GPU results against the FP64 oracle on a
-    sample of query points (checker only)."""
+    """Error of the GPU results against the FP64 oracle (FP64 hierarchize +
+    evaluate of the same nodal values) on `nsample` query points spread over
+    the launch (checker only).  max_rel_floor1e-3 is the per-point relative
+    error |u - u64| / max(|u64|, 1e-3 max|u64|)."""
     from oracle.oracle import Oracle
     wl = wl or single_workload()
     o = Oracle(wl["d"], wl["n"], wl["limits"])
@@ -217,39 +286,65 @@ def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsampl
     return res
 
 
-# ---------------------------------------------------------------------------
-def run_reference_arm(args, rank: int):
+def single_config(world: int, m: int, precision: str = "fp32") -> dict:
+    """`config` of the default workload's line (both arms)."""
+    return {"workload": WORKLOAD, "points_per_step_per_rank": m, "d": D, "n": NLEV, "limits": [NLEV - 1] * D,
+            "num_points": N_POINTS, "num_subspaces": N_SUBSPACES, "hier_precision": precision,
+            "l2": "inputs larger than L2 (132 MB grid + 671 MB points)",
+            "parallelism": f"grid replicated, points sharded over {world} rank(s)"}
+
+
+def repo_libraries() -> list:
+    """The in-repo shared libraries mapped into this process."""
+    libs = set()
+    try:
+        for ln in open("/proc/self/maps"):
+            path = ln.split()[-1] if ln.strip() else ""
+            if path.endswith(".so") and path.startswith(ROOT):
+                libs.add(os.path.relpath(path, ROOT))
+    except OSError:
+        pass
+    return sorted(libs)
+
+
+def run_reference_arm(args, rank: int, world: int):
+    """The reference's CPU implementation (oracle/_ref) on the default
+    workload; inputs come from the checker side (oracle/) only, so the
+    product library is never loaded.  Rank 0 alone runs."""
     if rank != 0:
-        return
+        return None
     if args.workload != "single":
         # the other workloads carry the reference's CPU time in their own
         # line (cpu_baseline / plain per-grid arms)
-        print(json.dumps({"impl": "reference", "workload": args.workload,
-                          "unavailable": "the reference arm times the default single-grid workload only"}))
-        return
-    from adaptive_sparse_grid_bench_b200 import Grid, inputs
-    g = Grid(D, NLEV)
-    vals = inputs.grid_values(g, inputs.f_gauss)
-    X = inputs.uniform_points(SEED, min(args.points or M_EVAL, 1 << 20), D)
-    vals_per = []
-    info = None
+        return {"impl": "reference", "workload": args.workload,
+                "unavailable": "the reference arm times the default single-grid workload only"}
+    from oracle import workload as owl
+    from oracle.oracle import Oracle
+    vals = owl.grid_values(Oracle(D, NLEV), owl.f_gauss)
+    m_step = args.points or M_EVAL
+    X = owl.uniform_points(SEED, min(m_step, 1 << 20), D)
+    rc = ReferenceCPU(D, NLEV, None, vals, X, m_step, cpu_step_seconds(args))
+    secs, rates = [], []
     for it in range(args.warmup + args.steps):
-        v, info = reference_cpu(vals, X, args.cpu_seconds)
+        t, v, _ = rc.step()
         if it >= args.warmup:
-            vals_per.append(v)
-    value = float(statistics.mean(vals_per))
-    line = {
-        "impl": "reference", "metric": "evals/s", "value": value, "unit": "evals/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * M_EVAL / value,
+            secs.append(t)
+            rates.append(v)
+    value = float(statistics.mean(rates))
+    sample = (f"per step: omp_hierarchize3 on the full grid + omp_evaluate5 on {rc.m} of {m_step} points; "
+              f"evals/s extrapolated linearly to {m_step} points")
+    return {
+        "impl": "reference", "metric": "evals/s", "value": value, "unit": "evals/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(statistics.mean(secs)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded SplitMix64)",
-        "config": {"workload": WORKLOAD, "points_per_step": M_EVAL, "l2": "inputs larger than L2"},
-        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": info["cores"], "kind": "reference",
-                         "sample": (f"omp_hierarchize3 on the full grid + omp_evaluate5 on "
-                                    f"{info['sample_points']} of 2^24 points, extrapolated linearly")},
+        "data": "synthetic (seeded SplitMix64)", "config": single_config(world, m_step),
+        "extrapolated_from_points": rc.m,
+        "ms_per_step_note": "measured time of one sampled step; value is extrapolated to the full step",
+        "libraries": repo_libraries(),
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": rc.cores, "kind": "reference",
+                         "sample": sample},
         "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
-    print(json.dumps(line), flush=True)
 
 
 def device_inputs(g, wl, rank, npts, torch, dev):
@@ -260,12 +355,67 @@ def device_inputs(g, wl, rank, npts, torch, dev):
     return vals, wl["points"](rank, npts)
 
 
-def run_b200(args, rank: int, world: int, local_rank: int, wl=None):
+class EventTimer:
+    """CUDA events on the launching stream around the timed steps."""
+
+    def __init__(self, stream):
+        import torch
+        self.stream = stream
+        self.e0 = torch.cuda.Event(enable_timing=True)
+        self.e1 = torch.cuda.Event(enable_timing=True)
+
+    def start(self):
+        self.e0.record(self.stream)
+
+    def stop(self):
+        self.e1.record(self.stream)
+
+    def ms(self) -> float:
+        self.e1.synchronize()
+        return self.e0.elapsed_time(self.e1)
+
+
+def timed_steps(step, steps: int, world: int, barrier, timer, device=None):
+    """The timed region every rank runs: barrier, `steps` calls of step()
+    between the timer's marks, barrier; returns (this rank's ms, the max over
+    ranks).  Every rank takes the same collective steps."""
+    from adaptive_sparse_grid_bench_b200.sharding import max_over_ranks
+    barrier()
+    timer.start()
+    for _ in range(steps):
+        step()
+    timer.stop()
+    barrier()
+    ms = timer.ms()
+    return ms, (max_over_ranks(ms, device) if world > 1 else ms)
+
+
+def job_rate(points_per_rank: int, world: int, steps: int, ms_max: float) -> float:
+    """Whole-job evals/s: every rank evaluates its own points each step
+    (weak scaling), the job's time is the slowest rank's."""
+    return world * points_per_rank * steps / (ms_max / 1e3)
+
+
+def rank_seed(base: int, rank: int, stride: int = 1) -> int:
+    """Rank r draws its query points from stream base + stride * r."""
+    return base + stride * rank
+
+
+def capture_figures():
+    """EVAL_CAPTURE while the evaluation source is the one it was measured on."""
+    import hashlib
+    try:
+        sha = hashlib.sha256(open(EVAL_SRC, "rb").read()).hexdigest()[:16]
+    except OSError:
+        sha = None
+    return (EVAL_CAPTURE if sha == EVAL_CAPTURE["source_sha16"] else None), sha
+
+
+def run_b200(args, rank: int, world: int, local_rank: int, wl=None, extras: bool = False, err: bool = False):
     import torch
     import torch.distributed as dist
     from adaptive_sparse_grid_bench_b200._lib import (SG_OPT_EVAL_PPT, SG_OPT_EVAL_SORT, SG_OPT_HIER_KERNEL,
-                                                      SG_OPT_PROFILE)
-    from adaptive_sparse_grid_bench_b200.sharding import max_over_ranks
+                                                      SG_OPT_PROFILE, kernel_launches)
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -284,11 +434,19 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None):
     tuned = g.autotune(X_d, out_d, m, stream)
     tuned["chosen"] = {"ppt": g.get_option(SG_OPT_EVAL_PPT), "sort": g.get_option(SG_OPT_EVAL_SORT),
                        "hier_kernel": g.get_option(SG_OPT_HIER_KERNEL)}
+    t_hier, t_eval, t_sort = [], [], []
 
     def step():
         g.set_values_device(vals_d, stream)
         g.hierarchize_async(stream)
         g.evaluate_device(X_d, out_d, m, stream)
+
+    def step_timed():
+        step()
+        t = g.timings()  # waits for this step's phase events
+        t_hier.append(t["hierarchize"])
+        t_sort.append(t["sort"])
+        t_eval.append(t["evaluate"])
 
     def barrier():
         if world > 1:
@@ -299,27 +457,12 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None):
         step()
     g.sync(stream)
     barrier()
-    t_hier, t_eval, t_sort = [], [], []
-    from adaptive_sparse_grid_bench_b200._lib import kernel_launches
     with Clocks(local_rank) as clk:
-        barrier()
         launches0 = kernel_launches()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            step()
-            t = g.timings()  # waits for this step's phase events
-            t_hier.append(t["hierarchize"])
-            t_sort.append(t["sort"])
-            t_eval.append(t["evaluate"])
-        e1.record(stream)
-        barrier()
+        ms, ms_max = timed_steps(step_timed, args.steps, world, barrier, EventTimer(stream), dev)
         launches = kernel_launches() - launches0
     g.sync(stream)
-    ms = e0.elapsed_time(e1)
-    ms_max = max_over_ranks(ms, dev) if world > 1 else ms
-    value = world * m * args.steps / (ms_max / 1e3)
+    value = job_rate(m, world, args.steps, ms_max)
 
     # end-to-end through the host-buffer C ABI, copies inside the timed region
     e2e = None
@@ -340,52 +483,60 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None):
 
         step_e2e()
         barrier()
-        s0 = torch.cuda.Event(enable_timing=True)
-        s1 = torch.cuda.Event(enable_timing=True)
-        s0.record()
-        for _ in range(args.steps):
-            step_e2e()
-        s1.record()
-        barrier()
-        e_ms = s0.elapsed_time(s1)
-        if world > 1:
-            e_ms = max_over_ranks(e_ms, dev)
-        e2e = {"value": world * m * args.steps / (e_ms / 1e3), "unit": "evals/s",
+        _, e_ms = timed_steps(step_e2e, args.steps, world, barrier, EventTimer(torch.cuda.current_stream()), dev)
+        e2e = {"value": job_rate(m, world, args.steps, e_ms), "unit": "evals/s",
                "h2d_bytes_per_step": int(g.num_points * 4 + m * D * 4), "d2h_bytes_per_step": int(m * 4)}
         if not np.array_equal(oh, out_d.cpu().numpy()):
             raise RuntimeError("host-buffer and device-pointer evaluations differ")
 
     if rank != 0:
-        return
+        return None
     S = g.num_subspaces
     hier_ms = statistics.mean(t_hier)
     eval_ms = statistics.mean(t_eval)
     hier_gbs = 8.0 * D * g.num_points / (hier_ms / 1e3) / 1e9
     peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
-        peak = float(json.load(open(peaks_path))["hbm_gbs"])
+        peaks = json.load(open(peaks_path))
+        peak = float(peaks["hbm_gbs"])
         peak_src = "measured"
     except (OSError, KeyError, ValueError):
-        peak, peak_src = 6650.0, "fallback"
+        peaks, peak, peak_src = {}, 6650.0, "fallback"
     eval_bytes = 4.0 * (S + D + 1) * m
     achieved = eval_bytes / (eval_ms / 1e3) / 1e9
     clocks = clk.summary()
+    pairs_per_s = m * S / (eval_ms / 1e3)
+    cap, src_sha = capture_figures()
+    default_case = wl["name"] == WORKLOAD and m == M_EVAL
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": cap["dram_bytes"] if (cap and default_case) else None,
+            "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch, captured "
+                               f"{cap['captured']} on evaluation source {cap['source_sha16']}") if cap else
+                              f"no capture for evaluation source {src_sha}",
+            "kernel": "k_evaluate", "peak_source": peak_src,
+            "bytes": "4*(S+d+1) per query point (cache-served surplus reads counted)"}
+    if cap:
+        # SM issue roofline: thread instructions per pair (ncu) x pairs/s
+        # against 148 SMs x 4 schedulers x one warp instruction per clock
+        mhz = clocks.get("sm_mhz") or float(peaks.get("sm_max_mhz", 1965.0))
+        issue = cap["inst_per_pair"] * pairs_per_s / 32.0
+        roof["issue"] = {"warp_inst_per_s": issue, "peak_warp_inst_per_s": SM_COUNT * SCHEDULERS_PER_SM * mhz * 1e6,
+                         "frac": issue / (SM_COUNT * SCHEDULERS_PER_SM * mhz * 1e6),
+                         "inst_per_pair": cap["inst_per_pair"]}
     line = {
         "metric": "evals/s", "value": value, "unit": "evals/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded SplitMix64; values sampled on device)",
-        "config": {"workload": wl["name"], "points_per_step_per_rank": m, "d": D, "n": g.n,
-                   "limits": [int(x) for x in g.limits], "num_points": g.num_points, "num_subspaces": S,
-                   "hier_precision": args.precision, "l2": wl["l2"], "parallelism": f"replicas x{world}",
-                   **wl["info"]},
-        "hierarchize": {"value": hier_gbs, "unit": "GB/s", "ms": hier_ms, "bytes": "8*d*N"},
+        "config": (single_config(world, m, args.precision) if wl["name"] == WORKLOAD else
+                   {"workload": wl["name"], "points_per_step_per_rank": m, "d": D, "n": g.n,
+                    "limits": [int(x) for x in g.limits], "num_points": g.num_points, "num_subspaces": S,
+                    "hier_precision": args.precision, "l2": wl["l2"],
+                    "parallelism": f"grid replicated, points sharded over {world} rank(s)", **wl["info"]}),
+        "hierarchize": {"value": hier_gbs, "unit": "GB/s", "ms": hier_ms, "bytes": "8*d*N",
+                        "frac_of_peak": hier_gbs / peak},
         "evaluate": {"ms": eval_ms, "sort_ms": statistics.mean(t_sort), "evals_per_s": m / (eval_ms / 1e3),
-                     "pairs_per_s": m * S / (eval_ms / 1e3)},
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": (EVAL_TRAFFIC_2P24 if wl["name"] == WORKLOAD and m == M_EVAL else None),
-                     "traffic_source": "ncu dram__bytes_read+write of one full launch (profiles/)",
-                     "kernel": "k_evaluate", "peak_source": peak_src,
-                     "bytes": "4*(S+d+1) per query point (cache-served surplus reads counted)"},
+                     "pairs_per_s": pairs_per_s},
+        "roofline": roof,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "autotune_ms": tuned,
@@ -393,13 +544,21 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None):
     }
     if world == 1 and not args.no_cpu_baseline:
         vals = vals_d.cpu().numpy()
-        cpu_v, info = reference_cpu(vals, X, args.cpu_seconds, wl)
-        line["cpu_baseline"] = {"value": cpu_v, "unit": "evals/s", "cores": info["cores"], "kind": "reference",
-                                "sample": (f"reference omp_hierarchize3 on the full grid + omp_evaluate5 on "
-                                           f"{info['sample_points']} of {wl['m_eval']} points, extrapolated "
-                                           f"linearly")}
+        cpu_v, info = reference_cpu(vals, X[:1 << 20], cpu_step_seconds(args), wl,
+                                    one_thread_points=4096 if extras else 0)
+        line["cpu_baseline"] = {
+            "value": cpu_v, "unit": "evals/s", "cores": info["cores"], "kind": "reference",
+            "sample": (f"reference omp_hierarchize3 on the full grid + omp_evaluate5 on {info['sample_points']} "
+                       f"of {wl['m_eval']} points, extrapolated linearly"),
+            "hierarchize_gbs": info["hierarchize_gbs"]}
+        if "one_thread" in info:
+            line["cpu_baseline"]["one_thread"] = info["one_thread"]
         line["err_vs_fp64"] = error_vs_fp64(vals, out_d.cpu().numpy(), X, ref_out=info["ref_out"], wl=wl)
-    print(json.dumps(line), flush=True)
+    elif world == 1 and err:
+        line["err_vs_fp64"] = error_vs_fp64(vals_d.cpu().numpy(), out_d.cpu().numpy(), X, nsample=256, wl=wl)
+    del X_d, out_d, vals_d
+    g.close()
+    return line
 
 
 def run_batched(args, rank: int, world: int, local_rank: int):
@@ -417,7 +576,7 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     from adaptive_sparse_grid_bench_b200.sharding import max_over_ranks
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    dims, levels, coef, counts = inputs.batch_workload(3 + rank, args.grids)
+    dims, levels, coef, counts = inputs.batch_workload(rank_seed(3, rank), args.grids)
     b = Batch(dims, levels)
     b.set_option(SG_OPT_HIER_PRECISION, SG_HIER_FP64 if args.precision == "fp64" else SG_HIER_FP32)
     b.set_option(SG_OPT_USE_GRAPH, 0 if args.no_graph else 1)
@@ -426,7 +585,7 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     b.get_values_device(vals)
     po = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
     nflt = int(np.sum(counts * dims))
-    X = torch.from_numpy(inputs.uniform01(SEED + 100 + rank, nflt)).to(dev)
+    X = torch.from_numpy(inputs.uniform01(rank_seed(SEED + 100, rank), nflt)).to(dev)
     out = torch.empty(int(po[-1]), dtype=torch.float32, device=dev)
     # a stream of its own: the legacy default stream cannot be captured, and
     # on this one the batch captures its launches once and replays the graphs
@@ -499,7 +658,7 @@ def run_batched(args, rank: int, world: int, local_rank: int):
         one.close()
     plain_value = plain_pts / (plain_ms / 1e3)
     if rank != 0:
-        return
+        return None
     err = None
     if world == 1 and not args.no_cpu_baseline:
         err = batch_error_vs_fp64(b, vals.cpu().numpy(), dims, levels, out.cpu().numpy(), xs, po, coff)
@@ -522,7 +681,8 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     }
     if err is not None:
         line["err_vs_fp64"] = err
-    print(json.dumps(line), flush=True)
+    b.close()
+    return line
 
 
 def batch_error_vs_fp64(b, nodal: np.ndarray, dims, levels, out: np.ndarray, xs: np.ndarray, po, coff,
@@ -531,7 +691,7 @@ def batch_error_vs_fp64(b, nodal: np.ndarray, dims, levels, out: np.ndarray, xs:
     for `per_d` grids of every dimension, FP64 hierarchization of the grid's
     nodal values and FP64 evaluation at `npts` of its query points."""
     from oracle.oracle import Oracle
-    worst_abs, worst_rel, checked = 0.0, 0.0, 0
+    worst_abs, worst_rel, worst_pt, checked = 0.0, 0.0, 0.0, 0
     for d in sorted(set(int(x) for x in dims)):
         for g in [int(i) for i in np.flatnonzero(dims == d)[:per_d]]:
             o = Oracle(d, int(levels[g]), None)
@@ -544,9 +704,37 @@ def batch_error_vs_fp64(b, nodal: np.ndarray, dims, levels, out: np.ndarray, xs:
             scale = max(float(np.max(np.abs(u64))), 1e-30)
             worst_abs = max(worst_abs, float(e.max()))
             worst_rel = max(worst_rel, float(e.max()) / scale)
+            worst_pt = max(worst_pt, float(np.max(e / np.maximum(np.abs(u64), 1e-3 * scale))))
             checked += 1
     return {"grids": checked, "points_per_grid": npts, "max_abs": worst_abs, "max_norm_rel": worst_rel,
+            "max_rel_floor1e-3": worst_pt,
             "note": "FP32 batched results vs FP64 hierarchize + evaluate of the same nodal values"}
+
+
+def served_error_vs_fp64(served, gsrc, dims, levels, coef, npts: int = 256):
+    """Served results against the FP64 oracle (checker only): each request's
+    grid is sampled again on the device (the same kernel the server used),
+    hierarchized and evaluated in FP64 at the request's first `npts` points."""
+    from adaptive_sparse_grid_bench_b200 import Grid
+    from adaptive_sparse_grid_bench_b200._lib import SG_FN_QUAD
+    from oracle.oracle import Oracle
+    worst_abs = worst_norm = worst_pt = 0.0
+    for gid, X, out in served:
+        k = gsrc[gid]
+        d, n = int(dims[k]), int(levels[k])
+        one = Grid(d, n)
+        one.sample_function(SG_FN_QUAD, coef[k, :3 * d])
+        nodal = one.get_values()
+        one.close()
+        o = Oracle(d, n)
+        u64 = o.evaluate_f64(o.hierarchize_f64(nodal.astype(np.float64)), X[:npts])
+        e = np.abs(out[:npts].astype(np.float64) - u64)
+        scale = max(float(np.max(np.abs(u64))), 1e-30)
+        worst_abs = max(worst_abs, float(e.max()))
+        worst_norm = max(worst_norm, float(e.max()) / scale)
+        worst_pt = max(worst_pt, float(np.max(e / np.maximum(np.abs(u64), 1e-3 * scale))))
+    return {"requests": len(served), "points_per_request": npts, "max_abs": worst_abs, "max_norm_rel": worst_norm,
+            "max_rel_floor1e-3": worst_pt}
 
 
 def run_served(args, rank: int, world: int, local_rank: int):
@@ -566,7 +754,7 @@ def run_served(args, rank: int, world: int, local_rank: int):
     from adaptive_sparse_grid_bench_b200._lib import SG_FN_QUAD, kernel_launches
     torch.cuda.set_device(local_rank)
     if rank != 0:
-        return
+        return None
     ngrid = args.pool
     dims, levels, coef, _ = inputs.batch_workload(4, ngrid)
     srv = Server(int(args.cap_gb * (1 << 30)), max_batch_points=max(args.batch_points, 65536))
@@ -574,6 +762,7 @@ def run_served(args, rank: int, world: int, local_rank: int):
     ids = [srv.add_grid(int(d), int(n), SG_FN_QUAD, coef[g, :3 * d]) for g, (d, n) in enumerate(zip(dims, levels))]
     admit_s = time.perf_counter() - t0
     gdim = {i: int(d) for i, d in zip(ids, dims)}
+    gsrc = {gid: k for k, gid in enumerate(ids)}  # grid id -> its workload entry
     resident = list(ids)
     pool = inputs.uniform01(40, 65536 * 12 * 4)  # query coordinates: slices of one uniform stream
     u = inputs.uniform01(4, 64 * args.requests + 4096)
@@ -619,6 +808,7 @@ def run_served(args, rank: int, world: int, local_rank: int):
                     continue
                 admit_ms.append(1e3 * (time.perf_counter() - a0))
                 gdim[nid] = int(dims[g])
+                gsrc[nid] = g
                 new_ids.append(nid)
 
         th = threading.Thread(target=admitter)
@@ -671,6 +861,7 @@ def run_served(args, rank: int, world: int, local_rank: int):
     # or within 1e-5 * max|u| + 2e-7 where the server split the sums
     from adaptive_sparse_grid_bench_b200 import SgError
     checked = bitwise = 0
+    served = []
     for kind, g, X in make_requests(64, 0.0):
         try:
             out, _ = srv.wait(srv.submit(g, X))
@@ -682,6 +873,8 @@ def run_served(args, rank: int, world: int, local_rank: int):
         if not np.all(err <= 1e-5 * max(float(np.max(np.abs(want))), 1e-30) + 2e-7):
             raise RuntimeError("served and plain results differ")
         checked += 1
+        served.append((g, X, out))
+    err64 = served_error_vs_fp64(served[:8], gsrc, dims, levels, coef)
 
     # the same kind of requests, one plain sg_evaluate call each (buffers warmed first)
     plain = []
@@ -718,36 +911,99 @@ def run_served(args, rank: int, world: int, local_rank: int):
         "plain_per_request": {"evals_per_s": plain_rate, "requests": len(plain),
                               "p50_ms": float(np.percentile(plat, 50)), "p99_ms": float(np.percentile(plat, 99))},
         "speedup_vs_plain": burst["evals_per_s"] / plain_rate, "checked_vs_plain": checked, "bitwise_vs_plain": bitwise,
-        "admit_ms_per_grid_initial": 1e3 * admit_s / ngrid, "server_stats": st,
+        "err_vs_fp64": err64, "admit_ms_per_grid_initial": 1e3 * admit_s / ngrid, "server_stats": st,
         "gpu_launches": int(launches), "clocks": clk.summary(),
     }
-    print(json.dumps(line), flush=True)
+    return line
+
+
+def free_port() -> int:
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def launch_ranks(n: int, argv) -> int:
+    """Starts this script as n local ranks (one process per GPU) through
+    torch.distributed.run and returns its exit status."""
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(free_port()), os.path.abspath(__file__), *argv]
+    env = dict(os.environ)
+    env.setdefault("NCCL_DEBUG", "INFO")  # the NCCL log names every rank of the communicator
+    return subprocess.call(cmd, env=env)
+
+
+def compact(line: dict | None, keys) -> dict | None:
+    return None if line is None else {k: line[k] for k in keys if k in line}
+
+
+def run_extras(args, rank: int, world: int, local_rank: int) -> dict:
+    """Short runs of the other workloads for the N=1 default line: the
+    batched step on 1024 grids, the served sweep at three rates with 1000
+    requests each, and the limits-adaptive grid; each with its error against
+    the FP64 oracle."""
+    import copy
+    out = {}
+    a = copy.copy(args)
+    a.steps, a.warmup = min(args.steps, 10), 3
+    a.grids = 1024
+    out["batched"] = compact(run_batched(a, rank, world, local_rank),
+                             ["value", "unit", "ms_per_step", "config", "hierarchize", "evaluate", "plain_per_grid",
+                              "speedup_vs_plain", "err_vs_fp64", "gpu_launches"])
+    a = copy.copy(args)
+    a.rates, a.requests = "2000,4000,8000", 1000
+    srv = run_served(a, rank, world, local_rank)
+    if srv is not None:
+        srv = compact(srv, ["value", "unit", "sweep", "burst", "best_rate_with_p99_le_2ms", "plain_per_request",
+                            "speedup_vs_plain", "checked_vs_plain", "bitwise_vs_plain", "err_vs_fp64"])
+        for r in srv.get("sweep", []) + [srv.get("burst") or {}]:
+            for k in ("creates", "admit_ms_mean", "rejected", "max_ms"):
+                r.pop(k, None)
+    out["served"] = srv
+    a = copy.copy(args)
+    a.steps, a.warmup, a.no_e2e, a.no_cpu_baseline, a.points = min(args.steps, 10), 3, True, True, None
+    out["adaptive"] = compact(run_b200(a, rank, world, local_rank, adaptive_workload(a), err=True),
+                              ["value", "unit", "ms_per_step", "config", "hierarchize", "evaluate", "err_vs_fp64",
+                               "gpu_launches"])
+    return out
 
 
 def main():
     args = parse()
+    if "WORLD_SIZE" not in os.environ and args.gpus > 1:
+        sys.exit(launch_ranks(args.gpus, sys.argv[1:]))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world != args.gpus:
+        raise SystemExit(f"--gpus {args.gpus} but {world} rank(s) were started")
     if args.impl == "reference":
-        run_reference_arm(args, rank)
+        line = run_reference_arm(args, rank, world)
+        if line is not None:
+            print(json.dumps(line), flush=True)
         return
     if world > 1:
         import datetime
         import torch
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
                                 device_id=torch.device("cuda", local_rank))
     try:
         if args.workload == "batched":
-            run_batched(args, rank, world, local_rank)
+            line = run_batched(args, rank, world, local_rank)
         elif args.workload == "served":
-            run_served(args, rank, world, local_rank)
+            line = run_served(args, rank, world, local_rank)
         elif args.workload == "adaptive":
-            run_b200(args, rank, world, local_rank, adaptive_workload(args))
+            line = run_b200(args, rank, world, local_rank, adaptive_workload(args))
         else:
-            run_b200(args, rank, world, local_rank)
+            extras = world == 1 and not args.no_extras
+            line = run_b200(args, rank, world, local_rank, extras=extras)
+            if line is not None and extras:
+                line.update(run_extras(args, rank, world, local_rank))
+        if line is not None:
+            print(json.dumps(line), flush=True)
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -69,6 +69,12 @@ extern "C" {
                                 /* sweeps of a group run back to back so it stays in  */
                                 /* L2; 0 = every sweep over the whole batch.  Set it  */
                                 /* before the batch's first device call.             */
+#define SG_OPT_TEST_WAIT 9      /* tests of the device-wait timeout, FP32 grids: k in */
+                                /* 1..2048 makes every staged sweep's first copy per  */
+                                /* CTA never start, so its bounded wait gives up after */
+                                /* k * 2^20 clock cycles (about k/2 ms); the next     */
+                                /* sg_sync returns SG_ERR_TIMEOUT and the values are  */
+                                /* invalid.  0 (default): off.                       */
 
 /* Phases reported by sg_timings (milliseconds of the most recent call). */
 #define SG_PHASE_HIERARCHIZE 0  /* all sweeps of the last hierarchization    */
@@ -133,7 +139,9 @@ int sg_evaluate_device(sg_grid *grid, const float *coord_mat, float *out,
  * make that first call before capturing work on the stream.  All
  * calls share the one array: calls whose work overlaps on the GPU (other
  * streams, other handles, other host threads) race and must be serialised
- * by the caller. */
+ * by the caller.  The looked-up address is cached per device (safe for
+ * concurrent host threads); a cudaDeviceReset invalidates it together with
+ * every handle on that device. */
 #define SG_NOALLOC_MAX_POINTS (1 << 18)
 #define SG_NOALLOC_SCRATCH_BYTES (24 << 20)
 int sg_evaluate_device_noalloc(sg_grid *grid, const float *coord_mat, float *out,

@@ -59,6 +59,8 @@ class Oracle:
             lib.or_hierarchize_f64_fast.argtypes = [C.c_void_p, _dp]
             lib.or_evaluate_f32.argtypes = [C.c_void_p, _fp, _fp, _fp, _i64]
             lib.or_evaluate_f64.argtypes = [C.c_void_p, _dp, _fp, _dp, _i64]
+            lib.or_evaluate_f64_par.argtypes = [C.c_void_p, _dp, _fp, _dp, _i64]
+            lib.or_evaluate_f64_par.restype = C.c_int
             lib.or_grid_points.argtypes = [C.c_void_p, _fp]
             cls._lib = lib
         return cls._lib
@@ -121,10 +123,18 @@ class Oracle:
         self.lib().or_evaluate_f32(self._buf, np.ascontiguousarray(surplus, np.float32), X, out, X.shape[0])
         return out
 
-    def evaluate_f64(self, surplus64, X) -> np.ndarray:
+    def evaluate_f64(self, surplus64, X, parallel: bool = True) -> np.ndarray:
+        """FP64 interpolant at the rows of X; `parallel` splits the points
+        over OpenMP threads with the subspaces' level vectors computed once
+        (bit-identical to the serial restatement)."""
         X = np.ascontiguousarray(X, np.float32).reshape(-1, self.d)
         out = np.zeros(X.shape[0], np.float64)
-        self.lib().or_evaluate_f64(self._buf, np.ascontiguousarray(surplus64, np.float64), X, out, X.shape[0])
+        a = np.ascontiguousarray(surplus64, np.float64)
+        if parallel and X.shape[0] > 1:
+            if self.lib().or_evaluate_f64_par(self._buf, a, X, out, X.shape[0]) != 0:
+                raise MemoryError("or_evaluate_f64_par")
+        else:
+            self.lib().or_evaluate_f64(self._buf, a, X, out, X.shape[0])
         return out
 
 

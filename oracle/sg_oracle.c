@@ -323,6 +323,63 @@ OR_API void or_evaluate_f64(const or_layout *L, const double *a, const float *X,
     }
 }
 
+/* or_evaluate_f64 for large grids and many points: the level vectors of all
+ * subspaces are computed once (memory order, as the loop above visits them)
+ * and the points are split over OpenMP threads.  Every point sees exactly
+ * the arithmetic of or_evaluate_f64, so the results are bit-identical. */
+OR_API int or_evaluate_f64_par(const or_layout *L, const double *a, const float *X,
+                               double *out, int64_t m)
+{
+    int d = L->d, s;
+    int64_t S = L->S, q = 0, pos, c;
+    int *lvs = (int *)malloc((size_t)S * (size_t)d * sizeof(int));
+    double *scs = (double *)malloc((size_t)S * (size_t)d * sizeof(double));
+    int64_t *bases = (int64_t *)malloc((size_t)S * sizeof(int64_t));
+    if (!lvs || !scs || !bases) {
+        free(lvs);
+        free(scs);
+        free(bases);
+        return -1;
+    }
+    {
+        int64_t base = 0;
+        for (s = 0; s < L->n; s++)
+            for (pos = 0; pos < L->dp[d - 1][s]; pos++, q++) {
+                int k;
+                or_idx2l(L, pos, s, lvs + q * d);
+                for (k = 0; k < d; k++) scs[q * d + k] = ldexp(1.0, lvs[q * d + k]);
+                bases[q] = base;
+                base += (int64_t)1 << s;
+            }
+    }
+#pragma omp parallel for schedule(dynamic, 4)
+    for (c = 0; c < m; c++) {
+        const float *x = X + c * d;
+        double acc = 0.0;
+        int64_t t2;
+        for (t2 = 0; t2 < S; t2++) {
+            const int *lv = lvs + t2 * d;
+            const double *sc = scs + t2 * d;
+            double prod = 1.0;
+            int64_t in_sub = 0;
+            int k;
+            for (k = 0; k < d; k++) {
+                double xs = (double)x[k] * sc[k];
+                int64_t t = (int64_t)xs;
+                double mm = 2.0 * (xs - (double)t) - 1.0;
+                in_sub = (in_sub << lv[k]) + t;
+                prod *= 1.0 - fabs(mm);
+            }
+            acc += prod * a[bases[t2] + in_sub];
+        }
+        out[c] = acc;
+    }
+    free(lvs);
+    free(scs);
+    free(bases);
+    return 0;
+}
+
 /* Coordinates of every grid point in compact order (N x d, row-major). */
 OR_API void or_grid_points(const or_layout *L, float *X)
 {

@@ -1,11 +1,15 @@
-"""Batches of grids on the GPU: bit-identical hierarchization to the
-single-grid path (and hence to hierarchize0), evaluation equal to the
-single-grid evaluation, in both precisions, with and without CUDA graphs."""
+"""Batches of grids on the GPU: hierarchization bit-identical to the oracle
+(FP32: hierarchize0, c:557-571; FP64: the FP64 oracle rounded once) and to
+the single-grid path, evaluation within conftest.check_eval's bounds of the
+FP64 oracle and equal to the single-grid evaluation, in both precisions,
+with and without CUDA graphs."""
 import numpy as np
 import pytest
 
 import adaptive_sparse_grid_bench_b200 as sg
 from adaptive_sparse_grid_bench_b200 import _lib, inputs
+from conftest import check_eval
+from oracle.oracle import Oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -80,6 +84,36 @@ def test_batch_evaluate_matches_single_grids(cuda, ppt, sort):
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"grid {g}"
 
 
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_batch_against_oracle(cuda, precision):
+    """Every grid of the mixed batch against the oracle directly: surpluses
+    bit for bit, evaluation of the batch's surpluses within tolerance of the
+    FP64 evaluation of the same surpluses."""
+    import torch
+    b = _batch(MIXED)
+    b.set_option(_lib.SG_OPT_HIER_PRECISION, _lib.SG_HIER_FP64 if precision == "fp64" else _lib.SG_HIER_FP32)
+    vals = inputs.uniform01(90, b.num_values) * 2 - 1
+    b.set_values(vals)
+    b.hierarchize()
+    surplus = b.get_values()
+    counts = [3, 1, 513, 1000, 257, 33, 2048, 600, 70, 511, 512, 1025]
+    po = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    Xs = [inputs.uniform_points(400 + g, counts[g], MIXED[g][0]) for g in range(len(MIXED))]
+    coords = torch.from_numpy(np.concatenate([x.reshape(-1) for x in Xs]).astype(np.float32)).to(cuda)
+    out = torch.full((int(po[-1]),), np.nan, device=cuda)
+    b.evaluate_device(po, coords, out)
+    b.sync()
+    res = out.cpu().numpy()
+    for g, (d, n, lim) in enumerate(MIXED):
+        o = Oracle(d, n, lim)
+        nodal = b.grid_values(vals, g)
+        want = (o.hierarchize_f32(nodal) if precision == "fp32"
+                else o.hierarchize_f64(nodal.astype(np.float64)).astype(np.float32))
+        got = b.grid_values(surplus, g)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"grid {g} ({d}, {n}, {lim})"
+        check_eval(res[po[g]:po[g + 1]], o.evaluate_f64(got.astype(np.float64), Xs[g]), f"grid {g}")
+
+
 def test_batch_sample_quad_and_config_like_workload(cuda):
     import torch
     dims, levels, coef, counts = inputs.batch_workload(3, 64, max_points=200_000)
@@ -95,14 +129,21 @@ def test_batch_sample_quad_and_config_like_workload(cuda):
     b.sync()
     res = out.cpu().numpy()
     for g in range(0, len(dims), 9):
-        one = sg.Grid(int(dims[g]), int(levels[g]))
-        one.sample_function(_lib.SG_FN_QUAD, coef[g, :3 * dims[g]])
+        d, n = int(dims[g]), int(levels[g])
+        one = sg.Grid(d, n)
+        one.sample_function(_lib.SG_FN_QUAD, coef[g, :3 * d])
         vals = one.get_values()
         one.hierarchize()
         assert np.array_equal(one.get_values().view(np.uint32), b.grid_values(surplus, g).view(np.uint32))
         want = one.evaluate(Xs[g])
         assert np.array_equal(res[po[g]:po[g + 1]].view(np.uint32), want.view(np.uint32))
         assert vals.size == b.grid_values(surplus, g).size
+        # and end to end against the oracle: hierarchize0's bits, and the
+        # FP32 results within tolerance of FP64 hierarchize + evaluate
+        o = Oracle(d, n)
+        assert np.array_equal(b.grid_values(surplus, g).view(np.uint32), o.hierarchize_f32(vals).view(np.uint32))
+        check_eval(res[po[g]:po[g + 1]], o.evaluate_f64(o.hierarchize_f64(vals.astype(np.float64)), Xs[g]),
+                   f"config-4 grid {g} (d={d}, n={n})")
 
 
 def test_batch_autotune_keeps_results(cuda):
