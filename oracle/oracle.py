@@ -17,6 +17,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libasgb_ref.so")
+REFCUDA_SO = os.path.join(HERE, "_ref", "libasgb_refcuda.so")
 
 _i64 = C.c_int64
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -209,3 +210,40 @@ class Reference:
             self.lib().ref_evaluate(variant, xs, o, xs.shape[0])
             out[s:s + chunk] = o
         return out
+
+
+class ReferenceCUDA:
+    """The reference's CUDA evaluate5 kernel (adaptive_sparse_grid_bench_cuda.cu:1522),
+    compiled in place (``_ref/libasgb_refcuda.so``); timed next to this
+    project's kernels.  The harness refuses sizes outside the kernel's safe
+    launch conditions (P a multiple of 32, points a multiple of 8 P, n <= 10,
+    d <= 20, coordinates in [0,1)) before touching the GPU."""
+
+    _lib = None
+
+    @classmethod
+    def available(cls) -> bool:
+        return os.path.exists(REFCUDA_SO)
+
+    @classmethod
+    def lib(cls) -> C.CDLL:
+        if cls._lib is None:
+            lib = _load(REFCUDA_SO)
+            lib.refcuda_evaluate5.argtypes = [C.c_int, C.c_int, _fp, C.c_int, _fp, C.c_int, C.c_int, C.c_int, _fp,
+                                              C.POINTER(C.c_float), C.POINTER(C.c_float)]
+            lib.refcuda_evaluate5.restype = C.c_int
+            cls._lib = lib
+        return cls._lib
+
+    @classmethod
+    def evaluate5(cls, d: int, n: int, surplus, X, points_per_warp: int, reps: int = 1):
+        """Returns (out, fastest kernel ms, fastest copy-inclusive ms)."""
+        a = np.ascontiguousarray(surplus, np.float32)
+        X = np.ascontiguousarray(X, np.float32).reshape(-1, d)
+        out = np.zeros(X.shape[0], np.float32)
+        tk, tt = C.c_float(), C.c_float()
+        r = cls.lib().refcuda_evaluate5(d, n, a, a.size, X, X.shape[0], points_per_warp, reps, out, C.byref(tk),
+                                        C.byref(tt))
+        if r != 0:
+            raise RuntimeError(f"refcuda_evaluate5 returned {r}")
+        return out, tk.value, tt.value

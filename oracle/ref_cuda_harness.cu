@@ -1,0 +1,126 @@
+/*
+ * Harness that compiles the REFERENCE CUDA benchmark in place and exports
+ * its evaluate5 kernel (adaptive_sparse_grid_bench_cuda.cu:1522-1598) for
+ * timing next to this project's kernels.  TEST INFRASTRUCTURE ONLY: built by
+ * oracle/Makefile into oracle/_ref/ (never committed); no reference source is
+ * copied into this repository; REF_CU names the file where it lies.
+ *
+ * Build-level adjustments, none of which changes the kernel:
+ *   - main() is renamed so the file links as a library;
+ *   - the reference passes symbol NAMES (strings) to cudaMemcpyToSymbol
+ *     (cu:1716-1717, cu:1772, cu:1793), which current CUDA rejects; the calls
+ *     are routed to a function that maps each name to its symbol.
+ *
+ * Launch conditions, checked before every launch (the kernel is never
+ * started otherwise):
+ *   - points per warp P a multiple of 32 and num_evals a multiple of 8 P:
+ *     evaluate5 calls __syncthreads inside `if (chunk < num_chunks)` and
+ *     `if (index < chunk_end)` (cu:1540-1572); with these sizes every thread
+ *     of every CTA takes both branches, so no barrier is divergent;
+ *   - n <= MAX_NUM_LEVELS (10) and d <= MAX_NUM_DIMS (20), the sizes of the
+ *     reference's constant tables (cu:17-18);
+ *   - coordinates in [0, 1), so every cell index t = (int)(x 2^l) lies in
+ *     its subspace.
+ * The reference's hierarchization kernels are not exported: lane 0 of each
+ * warp writes shared memory that the other lanes read with no __syncwarp
+ * (hierarchize7, cu:1080-1097, cu:1100-1108, cu:1155-1156), a race whose
+ * outcome can be an out-of-range index.
+ */
+#include <cuda_runtime.h>
+#include <stdlib.h>
+#include <string.h>
+
+static cudaError_t asgb_copy_to_symbol(const char *name, const void *src, size_t count);
+#define cudaMemcpyToSymbol(sym, src, count) asgb_copy_to_symbol(sym, src, count)
+#define main asgb_refcuda_main
+#include REF_CU
+#undef main
+#undef cudaMemcpyToSymbol
+
+static cudaError_t asgb_copy_to_symbol(const char *name, const void *src, size_t count)
+{
+    if (!strcmp(name, "d_dp_mat")) return cudaMemcpyToSymbol(d_dp_mat, src, count);
+    if (!strcmp(name, "d_lidx_vect")) return cudaMemcpyToSymbol(d_lidx_vect, src, count);
+    if (!strcmp(name, "d_par_lili")) return cudaMemcpyToSymbol(d_par_lili, src, count);
+    return cudaErrorInvalidSymbol;
+}
+
+#define REFCUDA_API extern "C" __attribute__((visibility("default")))
+
+/* Evaluates the hierarchized grid sg1d (N values, compact order) at m points
+ * (coords: m x d row-major, in [0,1)) with the reference's evaluate5, P
+ * points per warp, `reps` times; out gets the last run's results.
+ * ms_kernel: fastest kernel time; ms_total: fastest time of the reference's
+ * own timed region (coordinate copy in, kernel, result copy out; cu:1829-1897).
+ * Returns 0, -1 for sizes outside the launch conditions, -2 for a grid size
+ * mismatch, or a positive cudaError_t. */
+REFCUDA_API int refcuda_evaluate5(int d, int n, const float *sg1d, int N, const float *coords, int m, int P,
+                                  int reps, float *out, float *ms_kernel, float *ms_total)
+{
+    int Nref = 0, S = 0, r;
+    float *d_sg1d = NULL, *d_trans = NULL, *d_out = NULL, *h_trans = NULL;
+    cudaEvent_t t0 = NULL, t1 = NULL, k0 = NULL, k1 = NULL;
+    cudaError_t e = cudaSuccess;
+    if (d < 1 || d > MAX_NUM_DIMS || n < 1 || n > MAX_NUM_LEVELS || P < 32 || P % 32 != 0 || m < 8 * P ||
+        m % (8 * P) != 0 || reps < 1)
+        return -1;
+    for (r = 0; r < m * d; r++)
+        if (!(coords[r] >= 0.0f && coords[r] < 1.0f)) return -1;
+    memset(h_dp_mat, 0, sizeof(h_dp_mat)); /* init_dp_mat accumulates into it */
+    memset(h_lidx_vect, 0, sizeof(h_lidx_vect));
+    init_restr_vec(d, n);
+    init_dp_mat(d, n);
+    init_lidx_vect(d, n, &Nref, &S);
+    if (Nref != N) return -2;
+    const size_t tbytes = (size_t)((m + WARP_SIZE - 1) / WARP_SIZE) * WARP_SIZE * d * sizeof(float);
+    const int num_threads = 256;
+    const int num_blocks = (m * WARP_SIZE) / (P * num_threads); /* exact: m % (8 P) == 0 */
+    const size_t smem = d * sizeof(int) + 2 * d * sizeof(float) + (d + 1) * sizeof(int);
+    h_trans = init_coord_mat_trans(d, m, (float *)coords);
+#define CK(x)                            \
+    do {                                 \
+        e = (x);                         \
+        if (e != cudaSuccess) goto done; \
+    } while (0)
+    CK(cudaMemcpyToSymbol(d_dp_mat, h_dp_mat, d * n * sizeof(int)));
+    CK(cudaMemcpyToSymbol(d_lidx_vect, h_lidx_vect, n * sizeof(int)));
+    CK(cudaMalloc(&d_sg1d, (size_t)N * sizeof(float)));
+    CK(cudaMalloc(&d_trans, tbytes));
+    CK(cudaMalloc(&d_out, (size_t)m * sizeof(float)));
+    CK(cudaMemcpy(d_sg1d, sg1d, (size_t)N * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventCreate(&k0));
+    CK(cudaEventCreate(&k1));
+    CK(cudaFuncSetCacheConfig(evaluate5, cudaFuncCachePreferL1));
+    *ms_kernel = *ms_total = -1.0f;
+    for (r = 0; r < reps; r++) {
+        float tk = 0.0f, tt = 0.0f;
+        CK(cudaEventRecord(t0, 0));
+        CK(cudaMemcpy(d_trans, h_trans, tbytes, cudaMemcpyHostToDevice));
+        CK(cudaMemset(d_out, 0, (size_t)m * sizeof(float)));
+        CK(cudaEventRecord(k0, 0));
+        evaluate5<<<num_blocks, num_threads, smem>>>(d, n, d_sg1d, d_trans, d_out, m, P);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(k1, 0));
+        CK(cudaDeviceSynchronize());
+        CK(cudaMemcpy(out, d_out, (size_t)m * sizeof(float), cudaMemcpyDeviceToHost));
+        CK(cudaEventRecord(t1, 0));
+        CK(cudaEventSynchronize(t1));
+        CK(cudaEventElapsedTime(&tk, k0, k1));
+        CK(cudaEventElapsedTime(&tt, t0, t1));
+        if (*ms_kernel < 0.0f || tk < *ms_kernel) *ms_kernel = tk;
+        if (*ms_total < 0.0f || tt < *ms_total) *ms_total = tt;
+    }
+#undef CK
+done:
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    if (k0) cudaEventDestroy(k0);
+    if (k1) cudaEventDestroy(k1);
+    cudaFree(d_sg1d);
+    cudaFree(d_trans);
+    cudaFree(d_out);
+    free(h_trans);
+    return e == cudaSuccess ? 0 : (int)e;
+}

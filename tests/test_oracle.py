@@ -99,3 +99,21 @@ def test_reference_variants_agree_on_regular_grid():
     assert np.array_equal(r.values(), h0)
     X = np.random.default_rng(3).random((1000, 5), dtype=np.float32)
     assert np.array_equal(r.evaluate(X, 7), r.evaluate(X, 0))
+
+
+def test_reference_cuda_harness_refuses_unsafe_sizes():
+    # every refusal happens on the host, before any CUDA call
+    from oracle.oracle import ReferenceCUDA
+    if not ReferenceCUDA.available():
+        pytest.skip("reference CUDA harness not built (reference sources absent)")
+    surplus = np.zeros(49, np.float32)  # d=2, n=4
+    X = np.full((256, 2), 0.5, np.float32)
+    X21 = np.full((256, 21), 0.5, np.float32)
+    for args in ((2, 4, surplus, X, 33), (2, 4, surplus, X[:100], 32), (2, 11, surplus, X, 32),
+                 (21, 4, surplus, X21, 32)):
+        with pytest.raises(RuntimeError, match="returned -1"):
+            ReferenceCUDA.evaluate5(*args)
+    Y = X.copy()
+    Y[3, 1] = 1.0
+    with pytest.raises(RuntimeError, match="returned -1"):
+        ReferenceCUDA.evaluate5(2, 4, surplus, Y, 32)
