@@ -33,6 +33,8 @@ SG_OPT_PROFILE = 6
 SG_OPT_USE_GRAPH = 7
 SG_OPT_SWEEP_GROUP = 8
 SG_OPT_TEST_WAIT = 9
+SG_SRV_OPT_ZERO_COPY = 1
+SG_SRV_OPT_HEAVY_PAIRS = 2
 SG_NUM_PHASES = 3
 
 SG_FN_REFERENCE = 0
@@ -107,6 +109,8 @@ SIGNATURES = {
     "sg_server_add_grid": (_i, [_p, _i, _i, _p, _i, _p, _i, _pi64]),
     "sg_server_submit": (_i, [_p, _i64, _p, _i64, _p, _pi64]),
     "sg_server_wait": (_i, [_p, _i64, C.POINTER(C.c_double)]),
+    "sg_server_wait_detail": (_i, [_p, _i64, _p]),
+    "sg_server_set_option": (_i, [_p, _i, _i64]),
     "sg_server_stats": (_i, [_p, _p]),
     "sg_server_evaluate_now": (_i, [_p, _i64, _p, _i64, _p]),
     "sg_last_error": (C.c_char_p, []),

@@ -48,12 +48,15 @@
 #include "sg_kernels.h"
 
 #define SG_API __attribute__((visibility("default")))
-#define SRV_SLOTS 2
+#define SRV_SLOTS 4               /* slots 0-1: light lane, 2-3: heavy lane */
+#define SRV_LANE_SLOTS 2
+#define SRV_HEAVY_PAIRS ((int64_t)1 << 27) /* default SG_SRV_OPT_HEAVY_PAIRS */
 #define SRV_MAX_REQS 8192 /* requests per batch */
 #define SRV_CTA_THREADS 256
 #define SRV_SPLIT_SUBSPACES 4096  /* grids (d >= 4) with this many subspaces get split sums */
 #define SRV_PART_SUBSPACES 2048   /* about this many subspaces per part (at most 8 parts) */
 #define SRV_LONG_CHAIN 2048       /* launches with a part this long use 1 point per thread */
+#define SRV_RING_BATCHES 4        /* the staging ring holds this many full batches */
 
 #define ARENA_ALIGN 256
 
@@ -183,9 +186,11 @@ typedef struct srv_req {
     const float *coords;
     float *out;
     int64_t m;
-    double t_submit, t_done;
+    double t_submit, t_take, t_launch, t_gpu, t_done; /* host clock, ms */
     int state; /* 0 queued, 1 running, 2 done, 3 failed */
     int64_t S;  /* subspaces of the grid (set when batched) */
+    int64_t ring_off; /* staged copy of the coordinates in the ring, -1: none */
+    int lane;         /* 0 light, 1 heavy (point x subspace pairs >= heavy_pairs) */
     sg_grid *g; /* the grid (set when batched) */
     struct srv_req *next;
 } srv_req;
@@ -196,6 +201,7 @@ typedef struct srv_slot {
     cudaEvent_t done, ev_in, ev_d[SG_MAX_DIMS + 1];
     int busy;
     float *h_coords, *h_out, *d_coords, *d_out;
+    float *m_coords, *m_out; /* device addresses of h_coords / h_out (mapped pinned memory) */
     sg_eval_args *h_args, *d_args;
     int32_t *h_items, *d_items;   /* evaluation CTAs, grouped by dimension */
     int32_t *h_citems, *d_citems; /* combine CTAs of the split requests     */
@@ -204,6 +210,9 @@ typedef struct srv_slot {
     int64_t out_off[SRV_MAX_REQS], coord_off[SRV_MAX_REQS], part_off[SRV_MAX_REQS];
     int order[SRV_MAX_REQS];
     int nreq;
+    double t_launch, t_gpu; /* launch_batch returned; completion seen */
+    int zero_copy;          /* the server's setting when the batch was taken */
+    int lane;               /* the queue this slot takes its batches from */
 } srv_slot;
 
 struct sg_server {
@@ -218,11 +227,21 @@ struct sg_server {
     int64_t next_id, cap_bytes;
     sg_arena arena; /* the cap, reserved once; every grid buffer lives here */
     uint64_t clock;
-    srv_req *head, *tail;
+    srv_req *head[2], *tail[2]; /* per lane */
     int64_t queued_points;
     srv_req **by_ticket;
     int64_t next_ticket, cap_tickets;
     int64_t max_points;
+    int zero_copy; /* SG_SRV_OPT_ZERO_COPY */
+    int64_t heavy_pairs; /* SG_SRV_OPT_HEAVY_PAIRS */
+    /* staging ring (pinned, mapped): submit copies a request's coordinates
+     * here in the caller's thread; allocations are freed in any order and
+     * reclaimed from the oldest */
+    char *ring, *ring_dev;
+    int64_t ring_size, ring_head, ring_tail;
+    int64_t *rq_off, *rq_size; /* live allocations in order (circular) */
+    char *rq_freed;
+    int64_t rq_first, rq_count, rq_cap;
     srv_slot slot[SRV_SLOTS];
     cudaStream_t admit_st;
     int64_t st_batches, st_requests, st_points, st_evictions, st_failed;
@@ -245,6 +264,57 @@ static double now_ms(void)
     return ts.tv_sec * 1e3 + ts.tv_nsec * 1e-6;
 }
 
+/* Reserves `bytes` (256-aligned) of the staging ring (lock held); returns
+ * the offset or -1 when the ring is full. */
+static int64_t ring_alloc(sg_server *s, int64_t bytes)
+{
+    int64_t off;
+    bytes = (bytes + 255) & ~(int64_t)255;
+    if (!s->ring || bytes > s->ring_size || s->rq_count == s->rq_cap) return -1;
+    if (s->rq_count == 0) {
+        s->ring_head = s->ring_tail = 0; /* empty */
+        off = 0;
+    } else if (s->ring_head > s->ring_tail) {
+        /* live range [tail, head): free are [head, size) and [0, tail) */
+        if (s->ring_size - s->ring_head >= bytes) off = s->ring_head;
+        else if (s->ring_tail >= bytes) off = 0;
+        else return -1;
+    } else {
+        /* wrapped: live [tail, size) and [0, head); free is [head, tail) */
+        if (s->ring_tail - s->ring_head >= bytes) off = s->ring_head;
+        else return -1;
+    }
+    {
+        const int64_t q = (s->rq_first + s->rq_count) % s->rq_cap;
+        s->rq_off[q] = off;
+        s->rq_size[q] = bytes;
+        s->rq_freed[q] = 0;
+        s->rq_count++;
+    }
+    s->ring_head = off + bytes;
+    return off;
+}
+
+/* Frees the allocation at `off` (lock held) and reclaims freed space from
+ * the oldest allocation on. */
+static void ring_free(sg_server *s, int64_t off)
+{
+    int64_t i;
+    for (i = 0; i < s->rq_count; i++) {
+        const int64_t q = (s->rq_first + i) % s->rq_cap;
+        if (!s->rq_freed[q] && s->rq_off[q] == off) {
+            s->rq_freed[q] = 1;
+            break;
+        }
+    }
+    while (s->rq_count > 0 && s->rq_freed[s->rq_first]) {
+        s->rq_first = (s->rq_first + 1) % s->rq_cap;
+        s->rq_count--;
+    }
+    if (s->rq_count > 0) s->ring_tail = s->rq_off[s->rq_first];
+    else s->ring_head = s->ring_tail = 0;
+}
+
 /* Delivers a finished batch (lock held; the results were copied into the
  * callers' buffers beforehand, outside the lock). */
 static void finish_slot(sg_server *s, srv_slot *sl, int ok)
@@ -253,8 +323,14 @@ static void finish_slot(sg_server *s, srv_slot *sl, int ok)
     int i;
     for (i = 0; i < sl->nreq; i++) {
         srv_req *r = sl->reqs[i];
+        r->t_gpu = sl->t_gpu;
+        r->t_launch = sl->t_launch;
         r->t_done = t;
         r->state = ok ? 2 : 3;
+        if (r->ring_off >= 0) {
+            ring_free(s, r->ring_off);
+            r->ring_off = -1;
+        }
         s->grids[r->gi].pins--;
         if (!ok) s->st_failed++;
     }
@@ -269,13 +345,15 @@ static int take_batch(sg_server *s, srv_slot *sl)
 {
     int64_t pts = 0, coff = 0, poff = 0;
     sl->nreq = 0;
-    while (s->head && sl->nreq < SRV_MAX_REQS) {
-        srv_req *r = s->head;
+    const int ln = sl->lane;
+    while (s->head[ln] && sl->nreq < SRV_MAX_REQS) {
+        srv_req *r = s->head[ln];
         if (sl->nreq > 0 && pts + r->m > s->max_points) break;
-        s->head = r->next;
-        if (!s->head) s->tail = NULL;
+        s->head[ln] = r->next;
+        if (!s->head[ln]) s->tail[ln] = NULL;
         s->queued_points -= r->m;
         r->state = 1;
+        r->t_take = now_ms();
         r->S = s->grids[r->gi].g->L.S;
         r->g = s->grids[r->gi].g; /* pinned: stays resident until delivered */
         sl->reqs[sl->nreq] = r;
@@ -309,12 +387,18 @@ static int launch_batch(sg_server *s, srv_slot *sl)
     int64_t coff = 0, pts = 0, ni = 0, nc = 0;
     int i, d, e, no = 0;
     int first[SG_MAX_DIMS + 1], count[SG_MAX_DIMS + 1], ppt[SG_MAX_DIMS + 1];
-    (void)s;
+    const int zc = sl->zero_copy; /* fixed for the batch when it was taken */
     for (i = 0; i < sl->nreq; i++) {
         srv_req *r = sl->reqs[i];
         int64_t p;
-        memcpy(sl->h_coords + sl->coord_off[i], r->coords, (size_t)(r->m * r->d) * sizeof(float));
-        sg_grid_eval_args(r->g, sl->d_coords + sl->coord_off[i], sl->d_out + sl->out_off[i], r->m, &sl->h_args[i]);
+        const float *dc;
+        if (zc && r->ring_off >= 0) {
+            dc = (const float *)(s->ring_dev + r->ring_off); /* staged at submit, read in place */
+        } else {
+            memcpy(sl->h_coords + sl->coord_off[i], r->coords, (size_t)(r->m * r->d) * sizeof(float));
+            dc = (zc ? sl->m_coords : sl->d_coords) + sl->coord_off[i];
+        }
+        sg_grid_eval_args(r->g, dc, (zc ? sl->m_out : sl->d_out) + sl->out_off[i], r->m, &sl->h_args[i]);
         if (sl->h_args[i].nparts > 1) {
             sl->h_args[i].part_out = sl->d_part + sl->part_off[i];
             for (p = 0; p < r->m; p += SRV_CTA_THREADS) {
@@ -352,7 +436,8 @@ static int launch_batch(sg_server *s, srv_slot *sl)
         }
         count[d] = (int)ni - first[d];
     }
-    if (cudaMemcpyAsync(sl->d_coords, sl->h_coords, (size_t)coff * 4, cudaMemcpyHostToDevice, sl->st) != cudaSuccess ||
+    if ((!zc &&
+         cudaMemcpyAsync(sl->d_coords, sl->h_coords, (size_t)coff * 4, cudaMemcpyHostToDevice, sl->st) != cudaSuccess) ||
         cudaMemcpyAsync(sl->d_args, sl->h_args, (size_t)sl->nreq * sizeof(sg_eval_args), cudaMemcpyHostToDevice,
                         sl->st) != cudaSuccess ||
         cudaMemcpyAsync(sl->d_items, sl->h_items, (size_t)ni * 8, cudaMemcpyHostToDevice, sl->st) != cudaSuccess ||
@@ -369,7 +454,8 @@ static int launch_batch(sg_server *s, srv_slot *sl)
             return SG_ERR_CUDA;
     }
     if (nc && sgk_combine_parts(sl->d_args, sl->d_citems, (int)nc, sl->st) != cudaSuccess) return SG_ERR_CUDA;
-    if (cudaMemcpyAsync(sl->h_out, sl->d_out, (size_t)pts * 4, cudaMemcpyDeviceToHost, sl->st) != cudaSuccess ||
+    if ((!zc &&
+         cudaMemcpyAsync(sl->h_out, sl->d_out, (size_t)pts * 4, cudaMemcpyDeviceToHost, sl->st) != cudaSuccess) ||
         cudaEventRecord(sl->done, sl->st) != cudaSuccess)
         return SG_ERR_CUDA;
     return SG_OK;
@@ -398,6 +484,7 @@ static void *dispatcher(void *arg)
             if (sl->busy == 1) {
                 cudaError_t q = cudaEventQuery(sl->done);
                 if (q == cudaSuccess) {
+                    sl->t_gpu = now_ms();
                     sl->busy = 2; /* delivering: not free, not polled */
                     pthread_mutex_unlock(&s->mu);
                     deliver(sl);
@@ -409,18 +496,21 @@ static void *dispatcher(void *arg)
                 }
             }
         }
+        /* light lane first: its slots run at the higher stream priority */
         for (i = 0; i < SRV_SLOTS; i++) {
             if (s->slot[i].busy) any_busy = 1;
-            else if (free_slot < 0) free_slot = i;
+            else if (free_slot < 0 && s->head[s->slot[i].lane]) free_slot = i;
         }
-        if (s->head && free_slot >= 0 && !s->fatal) {
+        if (free_slot >= 0 && !s->fatal) {
             srv_slot *sl = &s->slot[free_slot];
             take_batch(s, sl);
+            sl->zero_copy = s->zero_copy;
             sl->busy = 1;
             s->st_batches++;
             s->st_requests += sl->nreq;
             pthread_mutex_unlock(&s->mu);
             i = launch_batch(s, sl);
+            sl->t_launch = now_ms();
             pthread_mutex_lock(&s->mu);
             if (i != SG_OK) {
                 finish_slot(s, sl, 0);
@@ -448,17 +538,20 @@ static void *dispatcher(void *arg)
             int ok;
             pthread_mutex_unlock(&s->mu);
             ok = cudaEventSynchronize(s->slot[i].done) == cudaSuccess;
+            s->slot[i].t_gpu = now_ms();
             if (ok) deliver(&s->slot[i]);
             pthread_mutex_lock(&s->mu);
             finish_slot(s, &s->slot[i], ok);
         }
-    while (s->head) {
-        srv_req *r = s->head;
-        s->head = r->next;
-        r->state = 3;
-        s->grids[r->gi].pins--;
+    for (int ln = 0; ln < 2; ln++) {
+        while (s->head[ln]) {
+            srv_req *r = s->head[ln];
+            s->head[ln] = r->next;
+            r->state = 3;
+            s->grids[r->gi].pins--;
+        }
+        s->tail[ln] = NULL;
     }
-    s->tail = NULL;
     pthread_cond_broadcast(&s->cv_done);
     pthread_mutex_unlock(&s->mu);
     return NULL;
@@ -506,6 +599,8 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
     }
     s->cap_bytes = hbm_cap_bytes;
     s->max_points = max_batch_points;
+    s->zero_copy = 1;
+    s->heavy_pairs = SRV_HEAVY_PAIRS;
     max_items = ((max_batch_points + SRV_CTA_THREADS - 1) / SRV_CTA_THREADS + SRV_MAX_REQS) * SG_EVAL_MAX_PARTS;
     pthread_mutex_init(&s->mu, NULL);
     pthread_mutex_init(&s->plain_mu, NULL);
@@ -519,10 +614,15 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
         srv_slot *sl = &s->slot[i];
         const size_t cb = (size_t)max_batch_points * SG_MAX_DIMS * 4, ob = (size_t)max_batch_points * 4;
         int ok = 1, d;
+        /* light batches at the highest priority, heavy ones one step below
+         * (still above admissions): as CTAs retire, light work takes SMs
+         * before the remaining CTAs of a heavy batch */
+        const int prio = i < SRV_LANE_SLOTS ? prio_high : (prio_high < prio_low ? prio_high + 1 : prio_high);
+        sl->lane = i < SRV_LANE_SLOTS ? 0 : 1;
         for (d = 1; d <= SG_MAX_DIMS && ok; d++)
-            ok = cudaStreamCreateWithPriority(&sl->dst[d], cudaStreamNonBlocking, prio_high) == cudaSuccess &&
+            ok = cudaStreamCreateWithPriority(&sl->dst[d], cudaStreamNonBlocking, prio) == cudaSuccess &&
                  cudaEventCreateWithFlags(&sl->ev_d[d], cudaEventDisableTiming) == cudaSuccess;
-        if (!ok || cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
+        if (!ok || cudaStreamCreateWithPriority(&sl->st, cudaStreamNonBlocking, prio) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl->done, cudaEventDisableTiming) != cudaSuccess ||
             cudaEventCreateWithFlags(&sl->ev_in, cudaEventDisableTiming) != cudaSuccess ||
             cudaMallocHost((void **)&sl->h_coords, cb) != cudaSuccess ||
@@ -534,7 +634,9 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
             cudaMalloc((void **)&sl->d_part, ob * SG_EVAL_MAX_PARTS) != cudaSuccess ||
             cudaMalloc((void **)&sl->d_coords, cb) != cudaSuccess || cudaMalloc((void **)&sl->d_out, ob) != cudaSuccess ||
             cudaMalloc((void **)&sl->d_args, SRV_MAX_REQS * sizeof(sg_eval_args)) != cudaSuccess ||
-            cudaMalloc((void **)&sl->d_items, (size_t)max_items * 8) != cudaSuccess) {
+            cudaMalloc((void **)&sl->d_items, (size_t)max_items * 8) != cudaSuccess ||
+            cudaHostGetDevicePointer((void **)&sl->m_coords, sl->h_coords, 0) != cudaSuccess ||
+            cudaHostGetDevicePointer((void **)&sl->m_out, sl->h_out, 0) != cudaSuccess) {
             cudaGetLastError();
             free_slots(s);
             free(s);
@@ -546,6 +648,21 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
         free_slots(s);
         free(s);
         return sfail(SG_ERR_CUDA, "sg_server_create: stream");
+    }
+    /* staging ring for zero-copy batches: room for SRV_RING_BATCHES full
+     * batches of 20-dimensional points (optional: without it, zero-copy
+     * batches stage in the dispatcher as the copying ones do) */
+    s->ring_size = SRV_RING_BATCHES * max_batch_points * SG_MAX_DIMS * (int64_t)sizeof(float);
+    s->rq_cap = SRV_RING_BATCHES * SRV_MAX_REQS;
+    s->rq_off = (int64_t *)malloc((size_t)s->rq_cap * sizeof(int64_t));
+    s->rq_size = (int64_t *)malloc((size_t)s->rq_cap * sizeof(int64_t));
+    s->rq_freed = (char *)malloc((size_t)s->rq_cap);
+    if (!s->rq_off || !s->rq_size || !s->rq_freed || cudaMallocHost((void **)&s->ring, (size_t)s->ring_size) != cudaSuccess ||
+        cudaHostGetDevicePointer((void **)&s->ring_dev, s->ring, 0) != cudaSuccess) {
+        cudaGetLastError();
+        if (s->ring) cudaFreeHost(s->ring);
+        s->ring = s->ring_dev = NULL;
+        s->ring_size = 0;
     }
     pthread_mutex_init(&s->arena.mu, NULL);
     s->arena.size = hbm_cap_bytes & ~(int64_t)(ARENA_ALIGN - 1);
@@ -593,6 +710,10 @@ SG_API int sg_server_destroy(sg_server *s)
     free(s->grids);
     cudaStreamDestroy(s->admit_st);
     free_slots(s);
+    if (s->ring) cudaFreeHost(s->ring);
+    free(s->rq_off);
+    free(s->rq_size);
+    free(s->rq_freed);
     cudaFree(s->arena.base);
     free(s->arena.fr);
     free(s->arena.live);
@@ -759,9 +880,18 @@ SG_API int sg_server_submit(sg_server *s, int64_t grid_id, const float *coord_ma
     r->t_submit = now_ms();
     s->grids[gi].pins++;
     s->grids[gi].last_used = ++s->clock;
-    if (s->tail) s->tail->next = r;
-    else s->head = r;
-    s->tail = r;
+    r->ring_off = s->zero_copy ? ring_alloc(s, num_evals * r->d * (int64_t)sizeof(float)) : -1;
+    if (r->ring_off >= 0) {
+        /* stage the coordinates in the caller's thread, outside the lock:
+         * the request is not queued yet, so nothing else reads the range */
+        pthread_mutex_unlock(&s->mu);
+        memcpy(s->ring + r->ring_off, coord_mat, (size_t)(num_evals * r->d) * sizeof(float));
+        pthread_mutex_lock(&s->mu);
+    }
+    r->lane = (double)num_evals * (double)s->grids[gi].g->L.S >= (double)s->heavy_pairs ? 1 : 0;
+    if (s->tail[r->lane]) s->tail[r->lane]->next = r;
+    else s->head[r->lane] = r;
+    s->tail[r->lane] = r;
     s->queued_points += num_evals;
     s->st_points += num_evals;
     *ticket = r->ticket;
@@ -771,6 +901,14 @@ SG_API int sg_server_submit(sg_server *s, int64_t grid_id, const float *coord_ma
 }
 
 SG_API int sg_server_wait(sg_server *s, int64_t ticket, double *latency_ms)
+{
+    double ms[5];
+    int r = sg_server_wait_detail(s, ticket, ms);
+    if (latency_ms) *latency_ms = ms[4];
+    return r;
+}
+
+SG_API int sg_server_wait_detail(sg_server *s, int64_t ticket, double *ms)
 {
     srv_req *r;
     int st;
@@ -782,11 +920,38 @@ SG_API int sg_server_wait(sg_server *s, int64_t ticket, double *latency_ms)
     }
     while (r->state < 2) pthread_cond_wait(&s->cv_done, &s->mu);
     st = r->state;
-    if (latency_ms) *latency_ms = r->t_done - r->t_submit;
+    if (ms) {
+        ms[0] = r->t_take - r->t_submit;
+        ms[1] = r->t_launch - r->t_submit;
+        ms[2] = r->t_gpu - r->t_submit;
+        ms[3] = (double)r->m * (double)r->S;
+        ms[4] = r->t_done - r->t_submit;
+    }
     s->by_ticket[ticket] = NULL;
     pthread_mutex_unlock(&s->mu);
     free(r);
     return st == 2 ? SG_OK : sfail(SG_ERR_CUDA, "sg_server_wait: the request failed");
+}
+
+SG_API int sg_server_set_option(sg_server *s, int option, int64_t value)
+{
+    if (!s) return sfail(SG_ERR_ARG, "sg_server_set_option: NULL server");
+    switch (option) {
+    case SG_SRV_OPT_ZERO_COPY:
+        if (value != 0 && value != 1) return sfail(SG_ERR_ARG, "SG_SRV_OPT_ZERO_COPY is 0 or 1");
+        pthread_mutex_lock(&s->mu);
+        s->zero_copy = (int)value;
+        pthread_mutex_unlock(&s->mu);
+        return SG_OK;
+    case SG_SRV_OPT_HEAVY_PAIRS:
+        if (value < 1) return sfail(SG_ERR_ARG, "SG_SRV_OPT_HEAVY_PAIRS is >= 1");
+        pthread_mutex_lock(&s->mu);
+        s->heavy_pairs = value;
+        pthread_mutex_unlock(&s->mu);
+        return SG_OK;
+    default:
+        return sfail(SG_ERR_ARG, "sg_server_set_option: unknown option %d", option);
+    }
 }
 
 SG_API int sg_server_stats(sg_server *s, int64_t *stats)

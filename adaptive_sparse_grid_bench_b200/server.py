@@ -33,6 +33,9 @@ class Server:
         except Exception:
             pass
 
+    def set_option(self, option: int, value: int) -> None:
+        check(L.lib().sg_server_set_option(self._h, int(option), int(value)))
+
     def add_grid(self, d: int, n: int, fn: int, params=(), limits=None) -> int:
         p = np.ascontiguousarray(params, np.float64)
         lim = None if limits is None else np.ascontiguousarray(limits, np.int32)
@@ -58,6 +61,17 @@ class Server:
         finally:
             _, out = self._keep.pop(ticket, (None, None))
         return out, lat.value
+
+    def wait_detail(self, ticket: int):
+        """(results, timeline): timeline = ms from submit to taken into a
+        batch, to launches issued, to completion seen, to results delivered,
+        and the request's point x subspace pairs."""
+        ms = np.zeros(5, np.float64)
+        try:
+            check(L.lib().sg_server_wait_detail(self._h, int(ticket), ms.ctypes.data))
+        finally:
+            _, out = self._keep.pop(ticket, (None, None))
+        return out, {"take_ms": ms[0], "launch_ms": ms[1], "gpu_ms": ms[2], "pairs": ms[3], "latency_ms": ms[4]}
 
     def evaluate_now(self, grid_id: int, coords: np.ndarray) -> np.ndarray:
         x = np.ascontiguousarray(coords, np.float32)

@@ -91,6 +91,13 @@ def parse():
     ap.add_argument("--create-frac", type=float, default=0.05, help="served: share of create+hierarchize requests")
     ap.add_argument("--batch-points", type=int, default=1 << 18, help="served: points per batch")
     ap.add_argument("--pool", type=int, default=512, help="served: resident grids at the start")
+    ap.add_argument("--zero-copy", type=int, default=None, choices=[0, 1],
+                    help="served: SG_SRV_OPT_ZERO_COPY (batches read and write pinned host memory in place)")
+    ap.add_argument("--heavy-pairs", type=int, default=None,
+                    help="served: SG_SRV_OPT_HEAVY_PAIRS (requests with this much work take the heavy lane)")
+    ap.add_argument("--served-dump", default=None,
+                    help="served: save each rate's per-request timeline (ms to batch, launch, completion, delivery; "
+                         "points; pairs) to PREFIX_<rate>.npy")
     return ap.parse_args()
 
 
@@ -758,6 +765,12 @@ def run_served(args, rank: int, world: int, local_rank: int):
     ngrid = args.pool
     dims, levels, coef, _ = inputs.batch_workload(4, ngrid)
     srv = Server(int(args.cap_gb * (1 << 30)), max_batch_points=max(args.batch_points, 65536))
+    if args.zero_copy is not None:
+        from adaptive_sparse_grid_bench_b200._lib import SG_SRV_OPT_ZERO_COPY
+        srv.set_option(SG_SRV_OPT_ZERO_COPY, args.zero_copy)
+    if args.heavy_pairs is not None:
+        from adaptive_sparse_grid_bench_b200._lib import SG_SRV_OPT_HEAVY_PAIRS
+        srv.set_option(SG_SRV_OPT_HEAVY_PAIRS, args.heavy_pairs)
     t0 = time.perf_counter()
     ids = [srv.add_grid(int(d), int(n), SG_FN_QUAD, coef[g, :3 * d]) for g, (d, n) in enumerate(zip(dims, levels))]
     admit_s = time.perf_counter() - t0
@@ -832,21 +845,30 @@ def run_served(args, rank: int, world: int, local_rank: int):
                 tickets.append((srv.submit(g, X), g, X))
             except Exception:
                 rejected += 1  # the grid was evicted after the request was drawn
-        lats, pts = [], 0
+        rows, pts = [], 0
         for t, g, X in tickets:
-            _, lat = srv.wait(t)
-            lats.append((lat, X.shape[0]))
+            _, tl = srv.wait_detail(t)
+            rows.append((tl["take_ms"], tl["launch_ms"], tl["gpu_ms"], tl["latency_ms"], X.shape[0], tl["pairs"]))
             pts += X.shape[0]
         wall = time.perf_counter() - start
         creates.put(None)
         th.join()
         resident.extend(new_ids)
-        lat = np.array([x for x, _ in lats])
-        small = np.array([x for x, m in lats if m <= 4096])
+        tl = np.array(rows, np.float64).reshape(-1, 6)
+        lat = tl[:, 3]
+        small = lat[tl[:, 4] <= 4096]
+        heavy = tl[:, 5] >= np.percentile(tl[:, 5], 90)  # the 10 % of requests with the most work
+        if args.served_dump:
+            np.save(f"{args.served_dump}_{rate if rate > 0 else 'burst'}.npy", tl)
+        pct = lambda a, q: float(np.percentile(a, q)) if a.size else None  # noqa: E731
         return {"rate_req_s": rate if rate > 0 else "burst", "requests": len(tickets), "rejected": rejected,
-                "evals_per_s": pts / wall, "p50_ms": float(np.percentile(lat, 50)),
-                "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
-                "p99_ms_le4096pts": float(np.percentile(small, 99)) if small.size else None,
+                "evals_per_s": pts / wall, "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "max_ms": float(lat.max()),
+                "p99_ms_le4096pts": pct(small, 99), "p99_ms_heaviest10pct": pct(lat[heavy], 99),
+                "p99_ms_other90pct": pct(lat[~heavy], 99),
+                "stages_p50_ms": {"queued": pct(tl[:, 0], 50), "staged": pct(tl[:, 1] - tl[:, 0], 50),
+                                  "device": pct(tl[:, 2] - tl[:, 1], 50), "delivered": pct(tl[:, 3] - tl[:, 2], 50)},
+                "stages_p99_ms": {"queued": pct(tl[:, 0], 99), "staged": pct(tl[:, 1] - tl[:, 0], 99),
+                                  "device": pct(tl[:, 2] - tl[:, 1], 99), "delivered": pct(tl[:, 3] - tl[:, 2], 99)},
                 "creates": len(new_ids), "admit_ms_mean": float(np.mean(admit_ms)) if admit_ms else None}
 
     sweep = []
@@ -905,7 +927,8 @@ def run_served(args, rank: int, world: int, local_rank: int):
         "config": {"workload": f"{ngrid} resident grids (d 2..12, n 3..9, <= 2e6 points), Poisson arrivals, "
                                f"{100 - 100 * args.create_frac:g}% evaluate (1..65536 log-uniform points), "
                                f"{100 * args.create_frac:g}% create+hierarchize", "cap_gb": args.cap_gb,
-                   "requests_per_rate": args.requests, "batch_points": max(args.batch_points, 65536)},
+                   "requests_per_rate": args.requests, "batch_points": max(args.batch_points, 65536),
+                   "zero_copy": args.zero_copy, "heavy_pairs": args.heavy_pairs},
         "sweep": sweep, "burst": burst,
         "best_rate_with_p99_le_2ms": best,
         "plain_per_request": {"evals_per_s": plain_rate, "requests": len(plain),

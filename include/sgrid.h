@@ -260,10 +260,12 @@ int sg_batch_device_bytes(const sg_batch *batch, int64_t *bytes);
 
 /* ---- serving loop --------------------------------------------------------
  * A pool of hierarchized grids resident on the current device under a byte
- * cap, and a dispatcher thread that batches evaluate requests continuously:
- * every request queued when a batch slot frees up goes into one batch (one
- * copy in, one batched launch per dimension, one copy out); two slots
- * alternate so one batch is assembled while the other computes.  No
+ * cap, and a dispatcher thread that batches evaluate requests continuously.
+ * Requests are queued in two lanes by their work (points x grid subspaces,
+ * SG_SRV_OPT_HEAVY_PAIRS); every request of a lane queued when one of the
+ * lane's two batch slots frees up goes into one batch (one batched launch
+ * per dimension), so one batch is assembled while the other computes, and
+ * light batches run at a higher stream priority than heavy ones.  No
  * reference counterpart. */
 typedef struct sg_server sg_server;
 /* max_batch_points: points per batch (and the largest single request).
@@ -287,6 +289,22 @@ int sg_server_submit(sg_server *server, int64_t grid_id, const float *coord_mat,
                      float *out, int64_t *ticket);
 /* Waits for a ticket; latency_ms (optional) = submit -> results in `out`. */
 int sg_server_wait(sg_server *server, int64_t ticket, double *latency_ms);
+/* sg_server_wait with the request's timeline, ms[5] (optional): milliseconds
+ * from submit until it was taken into a batch, until the batch's launches
+ * were issued, until the batch's completion was seen, the request's work in
+ * point x subspace pairs, and milliseconds until its results were in `out`. */
+int sg_server_wait_detail(sg_server *server, int64_t ticket, double *ms);
+/* Server options (sg_server_set_option). */
+#define SG_SRV_OPT_ZERO_COPY 1 /* 1 (default): batches read coordinates from and write
+                                  results to pinned host memory directly (no copy
+                                  stages; each request's coordinates are staged into a
+                                  pinned ring by sg_server_submit in the caller's
+                                  thread); 0: one copy in and one out per batch */
+#define SG_SRV_OPT_HEAVY_PAIRS 2 /* requests whose points x grid subspaces reach this
+                                    (default 2^27) queue in the heavy lane: its own
+                                    batches and slots at a lower stream priority, so
+                                    light requests never wait behind them */
+int sg_server_set_option(sg_server *server, int option, int64_t value);
 /* stats[7]: batches, requests, points, evictions, resident grids, bytes of
  * the reserved range in use, failed requests */
 int sg_server_stats(sg_server *server, int64_t *stats);

@@ -111,7 +111,8 @@ def test_batch_against_oracle(cuda, precision):
                 else o.hierarchize_f64(nodal.astype(np.float64)).astype(np.float32))
         got = b.grid_values(surplus, g)
         assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"grid {g} ({d}, {n}, {lim})"
-        check_eval(res[po[g]:po[g + 1]], o.evaluate_f64(got.astype(np.float64), Xs[g]), f"grid {g}")
+        # random nodal values: the norm-wise bound (conftest.check_eval)
+        check_eval(res[po[g]:po[g + 1]], o.evaluate_f64(got.astype(np.float64), Xs[g]), f"grid {g}", per_point=False)
 
 
 def test_batch_sample_quad_and_config_like_workload(cuda):

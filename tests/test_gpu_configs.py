@@ -17,7 +17,7 @@ Checks and tolerances (stated here, used below):
     on the same nodal values (hierarchize0 + evaluate0 restated in double,
     c:557-571, c:1237-1274), within conftest.check_eval's bounds:
       norm-wise   |u - u64| <= 1e-5 max|u64| + 2e-7,
-      per point   |u - u64| <= 1e-5 max(|u64|, 1e-3 max|u64|);
+      per point   |u - u64| <= 1e-5 max(|u64|, 1e-2 max|u64|);
   - the reference's own correctness check (c:2027-2029): at grid points the
     interpolant reproduces the sampled f within 1e-6.
 """

@@ -31,14 +31,16 @@ def assert_same_or_close(got, want, split):
     assert np.all(err <= RTOL_NORM * scale + ATOL), f"max err {err.max():.3e}"
 
 
-def _server(cap=8 << 30):
+def _server(cap=8 << 30, zero_copy=0):
     srv = sg.Server(cap, max_batch_points=1 << 18)
+    srv.set_option(_lib.SG_SRV_OPT_ZERO_COPY, zero_copy)
     ids = [srv.add_grid(d, n, fn, p) for d, n, fn, p in SHAPES]
     return srv, ids
 
 
-def test_server_results_equal_single_grid(cuda):
-    srv, ids = _server()
+@pytest.mark.parametrize("zero_copy", [0, 1])
+def test_server_results_equal_single_grid(cuda, zero_copy):
+    srv, ids = _server(zero_copy=zero_copy)
     rng_seed = 40
     tickets = []
     for q in range(40):
@@ -57,11 +59,13 @@ def test_server_results_equal_single_grid(cuda):
     srv.close()
 
 
+@pytest.mark.parametrize("zero_copy", [0, 1])
 @pytest.mark.parametrize("mine_g", [1, 5, 6])
-def test_same_result_alone_and_in_mix(cuda, mine_g):
+def test_same_result_alone_and_in_mix(cuda, mine_g, zero_copy):
     # bit for bit, split grids (5, 6) included: a grid's parts are fixed at
-    # admission, whatever else is in the batch
-    srv, ids = _server()
+    # admission, whatever else is in the batch; the same with the batches
+    # reading and writing pinned host memory in place
+    srv, ids = _server(zero_copy=zero_copy)
     X = inputs.uniform_points(7, 20000, SHAPES[mine_g][0])
     X[:3] = [[0.0] * X.shape[1], [1.0] * X.shape[1], [np.nan] * X.shape[1]]  # edges and NaN
     alone, _ = srv.wait(srv.submit(ids[mine_g], X))
@@ -185,4 +189,55 @@ def test_reserved_range_reused_across_evictions(cuda):
         st = srv.stats()
         assert st["bytes_in_use"] <= cap
     assert srv.stats()["evictions"] > 0 and srv.stats()["failed"] == 0
+    srv.close()
+
+
+def test_zero_copy_ring_wraps_and_matches(cuda):
+    """Many zero-copy requests in flight: the staging ring wraps around and
+    frees out of order; every result equals the copying path's."""
+    srv, ids = _server(zero_copy=1)
+    ref, _ = _server(zero_copy=0)
+    window = []
+
+    def check_oldest():
+        g, X, t = window.pop(0)
+        out, _ = srv.wait(t)
+        want, _ = ref.wait(ref.submit(ids[g], X))
+        assert np.array_equal(out.view(np.uint32), want.view(np.uint32))
+
+    for q in range(300):  # about 450 MB of coordinates through an 84 MB ring
+        g = q % len(ids)
+        m = 1 + (7919 * q) % 60000
+        X = inputs.uniform_points(500 + q, m, SHAPES[g][0])
+        window.append((g, X, srv.submit(ids[g], X)))
+        if len(window) > 24:
+            check_oldest()
+    while window:
+        check_oldest()
+    with pytest.raises(sg.SgError):
+        srv.set_option(_lib.SG_SRV_OPT_ZERO_COPY, 2)
+    srv.close()
+    ref.close()
+
+
+@pytest.mark.parametrize("heavy_pairs", [1, 1 << 22, 1 << 62])
+def test_lanes_keep_results(cuda, heavy_pairs):
+    """Requests split between the light and heavy lanes by their work give
+    the same results as the plain call, whichever lane they take (all heavy,
+    mixed, all light)."""
+    srv, ids = _server()
+    srv.set_option(_lib.SG_SRV_OPT_HEAVY_PAIRS, heavy_pairs)
+    tickets = []
+    for q in range(48):
+        g = (5 * q) % len(ids)
+        m = [3, 700, 5000, 40000][q % 4]
+        X = inputs.uniform_points(900 + q, m, SHAPES[g][0])
+        tickets.append((g, X, srv.submit(ids[g], X)))
+    for g, X, t in tickets:
+        out, _ = srv.wait(t)
+        d, n = SHAPES[g][:2]
+        assert_same_or_close(out, srv.evaluate_now(ids[g], X),
+                             d >= 4 and sg.Grid(d, n).num_subspaces >= SPLIT_SUBSPACES)
+    with pytest.raises(sg.SgError):
+        srv.set_option(_lib.SG_SRV_OPT_HEAVY_PAIRS, 0)
     srv.close()
