@@ -16,6 +16,10 @@ typedef sg_eval_args EvalArgs;
 template <int D>
 int eval_launch(const EvalArgs &A, int ppt, void *stream);
 
+/* Sets the kernels' dynamic shared memory limit on the current device. */
+template <int D>
+int eval_setup();
+
 /* Points per CTA of the evaluation kernels for `ppt` points per thread. */
 #define SG_EVAL_CTA_POINTS(ppt) (256 * (ppt))
 

@@ -3,4 +3,5 @@
 #include "eval_impl.cuh"
 
 template int eval_launch<12>(const EvalArgs &, int, void *);
+template int eval_setup<12>();
 template int eval_batch_launch<12>(const EvalArgs *, const int2 *, int, int, void *);

@@ -18,9 +18,15 @@
  *     base + coff(c) + t_c sub(R-c) + aoff(a) + t_a plen(a) + (2^b - 1 + t_b):
  *   - blocks follow each other in walk order, so the block base is a running
  *     counter plus one multiply-add per point (no table);
- *   - 2^b - 1 + t_b and the hats of dims A, B (and C for small budgets) are
- *     precomputed per point in registers, so each subspace costs one add,
- *     one gather and one FMA;
+ *   - 2^b - 1 + t_b and the hats of dim B are precomputed per point in
+ *     registers, the hats of dims A and C in this thread's column of shared
+ *     memory (registers held them before: 128 registers with spills), so
+ *     each subspace costs one add, one gather and one FMA;
+ *   - the two points of a thread are computed with Blackwell's packed FP32x2
+ *     instructions (FFMA2, FADD2, FMUL2 through __ffma2_rn, __fadd2_rn,
+ *     __fmul2_rn): one instruction does both points' FMA, product or
+ *     compensated add, with each point's rounding exactly as in scalar code,
+ *     so results are bit-identical to one point per thread;
  *   - blocks of budget R <= kRF run fully unrolled; larger blocks loop over
  *     their planes and run each plane's 2-D sub-block fully unrolled behind a
  *     jump table.  A block or sub-block whose budget is within the limits of
@@ -57,19 +63,52 @@ constexpr int kNB = 10; /* 2-D sub-blocks of budget r < kNB run fully unrolled *
 constexpr int kRF = 5;  /* 3-D blocks of budget R <= kRF run fully unrolled    */
 constexpr int kTB = 15; /* T = floor(x 2^15) holds the cells of levels 0..15   */
 
-__device__ __forceinline__ void kahan_add(float &s, float &c, float v)
+/* P floats of one thread's points: float2 (packed FP32x2 instructions) for
+ * P = 2, a plain float for P = 1. */
+template <int P>
+struct FV;
+template <>
+struct FV<1> {
+    float v;
+    __device__ __forceinline__ float get(int) const { return v; }
+    __device__ __forceinline__ void set(int, float x) { v = x; }
+    static __device__ __forceinline__ FV all(float x) { return FV{x}; }
+};
+template <>
+struct FV<2> {
+    float2 v;
+    __device__ __forceinline__ float get(int p) const { return p ? v.y : v.x; }
+    __device__ __forceinline__ void set(int p, float x)
+    {
+        if (p) v.y = x;
+        else v.x = x;
+    }
+    static __device__ __forceinline__ FV all(float x) { return FV{make_float2(x, x)}; }
+};
+__device__ __forceinline__ FV<1> vfma(FV<1> a, FV<1> b, FV<1> c) { return FV<1>{fmaf(a.v, b.v, c.v)}; }
+__device__ __forceinline__ FV<1> vmul(FV<1> a, FV<1> b) { return FV<1>{__fmul_rn(a.v, b.v)}; }
+__device__ __forceinline__ FV<1> vadd(FV<1> a, FV<1> b) { return FV<1>{__fadd_rn(a.v, b.v)}; }
+__device__ __forceinline__ FV<1> vsub(FV<1> a, FV<1> b) { return FV<1>{__fsub_rn(a.v, b.v)}; }
+__device__ __forceinline__ FV<2> vfma(FV<2> a, FV<2> b, FV<2> c) { return FV<2>{__ffma2_rn(a.v, b.v, c.v)}; }
+__device__ __forceinline__ FV<2> vmul(FV<2> a, FV<2> b) { return FV<2>{__fmul2_rn(a.v, b.v)}; }
+__device__ __forceinline__ FV<2> vadd(FV<2> a, FV<2> b) { return FV<2>{__fadd2_rn(a.v, b.v)}; }
+__device__ __forceinline__ FV<2> vsub(FV<2> a, FV<2> b)
 {
-    const float y = __fsub_rn(v, c);
-    const float t = __fadd_rn(s, y);
-    c = __fsub_rn(__fsub_rn(t, s), y);
+    return FV<2>{__fadd2_rn(a.v, make_float2(-b.v.x, -b.v.y))};
+}
+
+/* compensated (Kahan) s += v, c holding the running rounding error */
+template <int P>
+__device__ __forceinline__ void kahan_add(FV<P> &s, FV<P> &c, FV<P> v)
+{
+    const FV<P> y = vsub(v, c);
+    const FV<P> t = vadd(s, y);
+    c = vsub(vsub(t, s), y);
     s = t;
 }
 
 /* hat at the current level from the fractional part y = frac(x 2^l) */
-__device__ __forceinline__ float hat_of(float y)
-{
-    return 1.0f - fabsf(fmaf(2.0f, y, -1.0f));
-}
+__device__ __forceinline__ float hat_of(float y) { return 1.0f - fabsf(fmaf(2.0f, y, -1.0f)); }
 
 /* next level: y <- frac(2y) (exact), returns floor(2y) */
 __device__ __forceinline__ uint32_t step_y(float &y)
@@ -80,16 +119,27 @@ __device__ __forceinline__ uint32_t step_y(float &y)
     return (uint32_t)b;
 }
 
+template <int P>
+__device__ __forceinline__ FV<P> hats(const FV<P> &y)
+{
+    FV<P> h;
+#pragma unroll
+    for (int p = 0; p < P; ++p) h.set(p, hat_of(y.get(p)));
+    return h;
+}
+
 /* Per-point values of the three innermost dims. */
 template <int P>
 struct Inner {
-    float hB[P][kNB];     /* hat of dim B at level b                 */
+    FV<P> hB[kNB];        /* hat of dim B at level b                 */
     uint32_t cB[P][kNB];  /* heap index 2^b - 1 + t_b of dim B       */
-    float hA[P][kNB];     /* hat of dim A at level a                 */
-    float hC[P][kRF + 1]; /* hat of dim C at level c                 */
+    const FV<P> *sh;      /* this thread's hats of dims A, C in smem */
     uint32_t TA[P];       /* floor(x_A 2^15): t_a = TA >> (15 - a)   */
     uint32_t TC[P];       /* floor(x_C 2^15)                         */
+    __device__ __forceinline__ FV<P> hA(int a) const { return sh[a * kThreads]; }
+    __device__ __forceinline__ FV<P> hC(int c) const { return sh[(kNB + c) * kThreads]; }
 };
+constexpr int kHatSlots = kNB + kRF + 1;
 
 /* Regular shapes: blocks whose budget is within the innermost limits. */
 __host__ __device__ constexpr uint32_t plen_reg(int r, int a) { return (2u << (r - a)) - 1u; }
@@ -111,39 +161,36 @@ __host__ __device__ constexpr uint32_t coff_reg(int R, int c)
  * levels.  Returns sum_a hA[a] sum_b hB[b] alpha[...]. */
 template <int r, int P>
 __device__ __forceinline__ void block2_fixed(const float *__restrict__ alpha, const uint32_t (&base)[P],
-                                             const Inner<P> &in, float (&s)[P])
+                                             const Inner<P> &in, FV<P> &s)
 {
 #pragma unroll
     for (int a = 0; a <= r; ++a) {
         uint32_t rb[P];
-        float sr[P];
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-            rb[p] = base[p] + aoff_reg(r, a) + (in.TA[p] >> (kTB - a)) * plen_reg(r, a);
-            sr[p] = 0.0f;
+        for (int p = 0; p < P; ++p) rb[p] = base[p] + aoff_reg(r, a) + (in.TA[p] >> (kTB - a)) * plen_reg(r, a);
+        FV<P> sr = FV<P>::all(0.0f);
+#pragma unroll
+        for (int b = 0; b <= r - a; ++b) {
+            FV<P> v;
+#pragma unroll
+            for (int p = 0; p < P; ++p) v.set(p, __ldg(alpha + rb[p] + in.cB[p][b]));
+            sr = vfma(in.hB[b], v, sr);
         }
-#pragma unroll
-        for (int b = 0; b <= r - a; ++b)
-#pragma unroll
-            for (int p = 0; p < P; ++p)
-                sr[p] = fmaf(in.hB[p][b], __ldg(alpha + rb[p] + in.cB[p][b]), sr[p]);
-#pragma unroll
-        for (int p = 0; p < P; ++p) s[p] = (a == 0) ? in.hA[p][0] * sr[p] : fmaf(in.hA[p][a], sr[p], s[p]);
+        s = (a == 0) ? vmul(in.hA(0), sr) : vfma(in.hA(a), sr, s);
     }
 }
 
 /* planes C..R of a fully unrolled 3-D block of budget R */
 template <int R, int C, int P>
 __device__ __forceinline__ void block3_planes(const float *__restrict__ alpha, const uint32_t (&base)[P],
-                                              const Inner<P> &in, float (&s)[P])
+                                              const Inner<P> &in, FV<P> &s)
 {
     uint32_t sb[P];
-    float s2[P];
+    FV<P> s2;
 #pragma unroll
     for (int p = 0; p < P; ++p) sb[p] = base[p] + coff_reg(R, C) + (in.TC[p] >> (kTB - C)) * blk2_reg(R - C);
     block2_fixed<R - C, P>(alpha, sb, in, s2);
-#pragma unroll
-    for (int p = 0; p < P; ++p) s[p] = (C == 0) ? in.hC[p][0] * s2[p] : fmaf(in.hC[p][C], s2[p], s[p]);
+    s = (C == 0) ? vmul(in.hC(0), s2) : vfma(in.hC(C), s2, s);
     if constexpr (C < R) block3_planes<R, C + 1, P>(alpha, base, in, s);
 }
 
@@ -151,45 +198,52 @@ __device__ __forceinline__ void block3_planes(const float *__restrict__ alpha, c
 template <int P>
 __device__ __forceinline__ void block2_generic(const float *__restrict__ alpha, int r, int limA, int limB,
                                                const float (&xA)[P], const float (&xB)[P], bool hasA,
-                                               const uint32_t (&base)[P], float (&s)[P])
+                                               const uint32_t (&base)[P], FV<P> &s)
 {
     const int amax = min(r, limA);
     uint32_t aoff = 0;
-    float yA[P];
+    FV<P> yA;
     uint32_t tA[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-        yA[p] = xA[p];
+        yA.set(p, xA[p]);
         tA[p] = 0;
-        s[p] = 0.0f;
     }
+    s = FV<P>::all(0.0f);
     for (int a = 0; a <= amax; ++a) {
         if (a) {
 #pragma unroll
-            for (int p = 0; p < P; ++p) tA[p] = 2 * tA[p] + step_y(yA[p]);
+            for (int p = 0; p < P; ++p) {
+                float y = yA.get(p);
+                tA[p] = 2 * tA[p] + step_y(y);
+                yA.set(p, y);
+            }
         }
         const int rl = min(r - a, limB) + 1;
         const uint32_t plen = (1u << rl) - 1u;
-        float yB[P], sr[P];
+        FV<P> yB, sr = FV<P>::all(0.0f);
         uint32_t tB[P], rb[P];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
-            yB[p] = xB[p];
+            yB.set(p, xB[p]);
             tB[p] = 0;
-            sr[p] = 0.0f;
             rb[p] = base[p] + aoff + tA[p] * plen;
         }
         for (int b = 0; b < rl; ++b) {
             if (b) {
 #pragma unroll
-                for (int p = 0; p < P; ++p) tB[p] = 2 * tB[p] + step_y(yB[p]);
+                for (int p = 0; p < P; ++p) {
+                    float y = yB.get(p);
+                    tB[p] = 2 * tB[p] + step_y(y);
+                    yB.set(p, y);
+                }
             }
+            FV<P> v;
 #pragma unroll
-            for (int p = 0; p < P; ++p)
-                sr[p] = fmaf(hat_of(yB[p]), __ldg(alpha + rb[p] + (1u << b) - 1u + tB[p]), sr[p]);
+            for (int p = 0; p < P; ++p) v.set(p, __ldg(alpha + rb[p] + (1u << b) - 1u + tB[p]));
+            sr = vfma(hats(yB), v, sr);
         }
-#pragma unroll
-        for (int p = 0; p < P; ++p) s[p] = fmaf(hasA ? hat_of(yA[p]) : 1.0f, sr[p], s[p]);
+        s = vfma(hasA ? hats(yA) : FV<P>::all(1.0f), sr, s);
         aoff += (1u << a) * plen;
     }
 }
@@ -197,7 +251,7 @@ __device__ __forceinline__ void block2_generic(const float *__restrict__ alpha, 
 /* Sub-block of budget r: unrolled (r within the limits, r < kNB) or generic. */
 template <int D, int P>
 __device__ __forceinline__ void block2_any(const EvalArgs &A, int r, const Inner<P> &in, const float (&xA)[P],
-                                           const float (&xB)[P], const uint32_t (&base)[P], float (&s)[P])
+                                           const float (&xB)[P], const uint32_t (&base)[P], FV<P> &s)
 {
     if (D >= 2 && r <= A.lim2) {
         switch (r) {
@@ -216,7 +270,7 @@ __device__ __forceinline__ void block2_any(const EvalArgs &A, int r, const Inner
 template <int D, int P>
 __device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<P> &in, const float (&xC)[P],
                                           const float (&xA)[P], const float (&xB)[P], const uint32_t (&base)[P],
-                                          float (&s)[P])
+                                          FV<P> &s)
 {
     if constexpr (D >= 3) {
         if (R <= kRF && R <= A.lim3) {
@@ -233,27 +287,30 @@ __device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<
     /* plane loop; dim C is absent (limit 0) for d < 3 */
     const int cmax = D >= 3 ? min(R, A.lim[D >= 3 ? D - 3 : 0]) : 0;
     uint32_t coff = 0;
-    float yC[P];
+    FV<P> yC;
     uint32_t tC[P];
 #pragma unroll
     for (int p = 0; p < P; ++p) {
-        yC[p] = xC[p];
+        yC.set(p, xC[p]);
         tC[p] = 0;
-        s[p] = 0.0f;
     }
+    s = FV<P>::all(0.0f);
     for (int c = 0; c <= cmax; ++c) {
         if (c) {
 #pragma unroll
-            for (int p = 0; p < P; ++p) tC[p] = 2 * tC[p] + step_y(yC[p]);
+            for (int p = 0; p < P; ++p) {
+                float y = yC.get(p);
+                tC[p] = 2 * tC[p] + step_y(y);
+                yC.set(p, y);
+            }
         }
         const uint32_t sub = A.blk2[R - c];
         uint32_t sb[P];
-        float s2[P];
+        FV<P> s2;
 #pragma unroll
         for (int p = 0; p < P; ++p) sb[p] = base[p] + coff + tC[p] * sub;
         block2_any<D, P>(A, R - c, in, xA, xB, sb, s2);
-#pragma unroll
-        for (int p = 0; p < P; ++p) s[p] = fmaf(D >= 3 ? hat_of(yC[p]) : 1.0f, s2[p], s[p]);
+        s = vfma(D >= 3 ? hats(yC) : FV<P>::all(1.0f), s2, s);
         coff += (1u << c) * sub;
     }
 }
@@ -270,27 +327,46 @@ constexpr int kLG = 3;
  * grows with d; grids of more dims keep the loop) */
 constexpr int kMaxUnrollD = 12;
 
+/* next level of one prefix dim for every point: y doubles, the cell index
+ * takes the next bit */
+template <int P>
+__device__ __forceinline__ void step_all(FV<P> &y, uint32_t (&ix)[P])
+{
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+        float t = y.get(p);
+        ix[p] = 2 * ix[p] + step_y(t);
+        y.set(p, t);
+    }
+}
+
 /* Levels l = L..B of the last prefix dim and their 3-D blocks of budget
  * B - l, fully unrolled (every shape regular: B within the limits). */
 template <int D, int P, int B, int L>
-__device__ __forceinline__ void leaf_group(const EvalArgs &A, uint32_t &cur, const Inner<P> &in,
-                                           const float (&pin)[P], float (&y)[P], uint32_t (&ix)[P], float (&acc)[P])
+__device__ __forceinline__ void leaf_group(const EvalArgs &A, uint32_t &cur, const Inner<P> &in, const FV<P> &pin,
+                                           FV<P> &y, uint32_t (&ix)[P], FV<P> &acc)
 {
-    if constexpr (L > 0) {
-#pragma unroll
-        for (int p = 0; p < P; ++p) ix[p] = 2 * ix[p] + step_y(y[p]);
-    }
+    if constexpr (L > 0) step_all<P>(y, ix);
     constexpr int R = B - L;
     constexpr uint32_t blk = coff_reg(R, R + 1);
     uint32_t base[P];
-    float s[P];
+    FV<P> s;
 #pragma unroll
     for (int p = 0; p < P; ++p) base[p] = cur + ix[p] * blk;
     cur += blk << (A.nm1 - R);
     block3_planes<R, 0, P>(A.alpha, base, in, s);
-#pragma unroll
-    for (int p = 0; p < P; ++p) acc[p] = fmaf(pin[p] * hat_of(y[p]), s[p], acc[p]);
+    acc = vfma(vmul(pin, hats(y)), s, acc);
     if constexpr (L < B) leaf_group<D, P, B, L + 1>(A, cur, in, pin, y, ix, acc);
+}
+
+/* the coordinates of prefix dim K of this thread's points */
+template <int P>
+__device__ __forceinline__ FV<P> load_y(const float *sx, int K, int tid)
+{
+    FV<P> y;
+#pragma unroll
+    for (int p = 0; p < P; ++p) y.set(p, sx[(K * P + p) * kThreads + tid]);
+    return y;
 }
 
 /* Levels l = L..B of prefix dim K = D-5, each followed by the unrolled
@@ -298,25 +374,18 @@ __device__ __forceinline__ void leaf_group(const EvalArgs &A, uint32_t &cur, con
  * as in the walk). */
 template <int D, int K, int P, int B, int L>
 __device__ __forceinline__ void leaf_group2(const EvalArgs &A, const float *sx, int tid, uint32_t &cur,
-                                            const Inner<P> &in, const float (&pin)[P], float (&y)[P],
-                                            uint32_t (&ix)[P], float (&sum)[P], float (&comp)[P])
+                                            const Inner<P> &in, const FV<P> &pin, FV<P> &y, uint32_t (&ix)[P],
+                                            FV<P> &sum, FV<P> &comp)
 {
-    if constexpr (L > 0) {
-#pragma unroll
-        for (int p = 0; p < P; ++p) ix[p] = 2 * ix[p] + step_y(y[p]);
-    }
-    float pn[P], y2[P], acc[P];
+    if constexpr (L > 0) step_all<P>(y, ix);
+    const FV<P> pn = vmul(pin, hats(y));
+    FV<P> y2 = load_y<P>(sx, K + 1, tid);
+    FV<P> acc = FV<P>::all(0.0f);
     uint32_t ix2[P];
 #pragma unroll
-    for (int p = 0; p < P; ++p) {
-        pn[p] = pin[p] * hat_of(y[p]);
-        y2[p] = sx[((K + 1) * P + p) * kThreads + tid];
-        ix2[p] = ix[p];
-        acc[p] = 0.0f;
-    }
+    for (int p = 0; p < P; ++p) ix2[p] = ix[p];
     leaf_group<D, P, B - L, 0>(A, cur, in, pn, y2, ix2, acc);
-#pragma unroll
-    for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], acc[p]);
+    kahan_add(sum, comp, acc);
     if constexpr (L < B) leaf_group2<D, K, P, B, L + 1>(A, sx, tid, cur, in, pin, y, ix, sum, comp);
 }
 
@@ -326,18 +395,15 @@ template <int D, int K, int P, bool SPLIT>
 struct Walk {
     static __device__ __forceinline__ void run(const EvalArgs &A, const float *sx, int tid, int budget,
                                                uint32_t &cur, Range &rg, const Inner<P> &in, const float (&xC)[P],
-                                               const float (&xA)[P], const float (&xB)[P], const float (&pin)[P],
-                                               const uint32_t (&ixin)[P], float (&sum)[P], float (&comp)[P])
+                                               const float (&xA)[P], const float (&xB)[P], const FV<P> &pin,
+                                               const uint32_t (&ixin)[P], FV<P> &sum, FV<P> &comp)
     {
         const int lmax = min(A.lim[K], budget);
-        float y[P], acc[P];
+        FV<P> y = load_y<P>(sx, K, tid);
+        FV<P> acc = FV<P>::all(0.0f);
         uint32_t ix[P];
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-            y[p] = sx[(K * P + p) * kThreads + tid];
-            ix[p] = ixin[p];
-            acc[p] = 0.0f;
-        }
+        for (int p = 0; p < P; ++p) ix[p] = ixin[p];
         if constexpr (D <= kMaxUnrollD && K + 1 == D - 4) {
             if (!(SPLIT && rg.partial) && budget <= 3 && budget <= A.lim[K] && budget <= A.lim[K + 1] &&
                 budget <= A.lim3) {
@@ -360,16 +426,12 @@ struct Walk {
                 case 3: leaf_group<D, P, 3, 0>(A, cur, in, pin, y, ix, acc); break;
                 default: break;
                 }
-#pragma unroll
-                for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], acc[p]);
+                kahan_add(sum, comp, acc);
                 return;
             }
         }
         for (int l = 0; l <= lmax; ++l) {
-            if (l) {
-#pragma unroll
-                for (int p = 0; p < P; ++p) ix[p] = 2 * ix[p] + step_y(y[p]);
-            }
+            if (l) step_all<P>(y, ix);
             if (SPLIT && rg.partial) {
                 /* the child subtree (depth K+1, budget - l) holds blocks
                  * [leaf, leaf + nb): skip it whole when outside [lo, hi) */
@@ -381,40 +443,33 @@ struct Walk {
                     continue;
                 }
             }
-            float pn[P];
-#pragma unroll
-            for (int p = 0; p < P; ++p) pn[p] = pin[p] * hat_of(y[p]);
+            const FV<P> pn = vmul(pin, hats(y));
             if constexpr (K == D - 4) {
                 const int R = budget - l;
                 const uint32_t blk = A.blk3[R];
                 uint32_t base[P];
-                float s[P];
+                FV<P> s;
 #pragma unroll
                 for (int p = 0; p < P; ++p) base[p] = cur + ix[p] * blk;
                 cur += blk << (A.nm1 - R);
                 if (SPLIT) ++rg.leaf;
                 block_sum<D, P>(A, R, in, xC, xA, xB, base, s);
-#pragma unroll
-                for (int p = 0; p < P; ++p) acc[p] = fmaf(pn[p], s[p], acc[p]);
+                acc = vfma(pn, s, acc);
             } else {
                 Walk<D, K + 1, P, SPLIT>::run(A, sx, tid, budget - l, cur, rg, in, xC, xA, xB, pn, ix, sum, comp);
             }
         }
-        if constexpr (K == D - 4) {
-#pragma unroll
-            for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], acc[p]);
-        }
+        if constexpr (K == D - 4) kahan_add(sum, comp, acc);
     }
 };
 
 /* Evaluates this thread's points first, first + 32, ..., first + 32(P-1)
  * (those below `end`) against grid A; sx is this CTA's shared coordinate
- * buffer. */
+ * buffer, shat its shared hats of dims A and C. */
 template <int D, int P, bool SPLIT>
-__device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int tid, int64_t first, int64_t end,
-                                            int part)
+__device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, FV<P> *shat, int tid, int64_t first,
+                                            int64_t end, int part)
 {
-
     float xC[P], xA[P], xB[P];
     bool valid[P], nan_in[P];
 #pragma unroll
@@ -446,6 +501,8 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int ti
     }
 
     Inner<P> in;
+    in.sh = shat + tid;
+    FV<P> *const shw = shat + tid;
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         float y = xB[p];
@@ -453,40 +510,50 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int ti
 #pragma unroll
         for (int j = 0; j < kNB; ++j) {
             if (j) t = 2 * t + step_y(y);
-            in.hB[p][j] = hat_of(y);
+            in.hB[j].set(p, hat_of(y));
             in.cB[p][j] = ((1u << j) - 1u) + t;
         }
         in.TA[p] = (uint32_t)(xA[p] * (float)(1u << kTB));
-        y = xA[p];
+        in.TC[p] = (uint32_t)(xC[p] * (float)(1u << kTB));
+    }
+    {
+        FV<P> yA, yC;
+#pragma unroll
+        for (int p = 0; p < P; ++p) {
+            yA.set(p, xA[p]);
+            yC.set(p, xC[p]);
+        }
 #pragma unroll
         for (int j = 0; j < kNB; ++j) {
-            if (j) (void)step_y(y);
-            in.hA[p][j] = hat_of(y);
+            if (j)
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    float y = yA.get(p);
+                    (void)step_y(y);
+                    yA.set(p, y);
+                }
+            shw[j * kThreads] = hats(yA);
         }
-        in.TC[p] = (uint32_t)(xC[p] * (float)(1u << kTB));
-        y = xC[p];
 #pragma unroll
         for (int j = 0; j <= kRF; ++j) {
-            if (j) (void)step_y(y);
-            in.hC[p][j] = hat_of(y);
+            if (j)
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    float y = yC.get(p);
+                    (void)step_y(y);
+                    yC.set(p, y);
+                }
+            shw[(kNB + j) * kThreads] = hats(yC);
         }
     }
 
-    float sum[P], comp[P];
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-        sum[p] = 0.0f;
-        comp[p] = 0.0f;
-    }
+    FV<P> sum = FV<P>::all(0.0f), comp = FV<P>::all(0.0f);
     uint32_t cur = 0;
     if constexpr (D >= 4) {
-        float pin[P];
+        const FV<P> pin = FV<P>::all(1.0f);
         uint32_t ix[P];
 #pragma unroll
-        for (int p = 0; p < P; ++p) {
-            pin[p] = 1.0f;
-            ix[p] = 0;
-        }
+        for (int p = 0; p < P; ++p) ix[p] = 0;
         Range rg;
         rg.leaf = 0;
         rg.partial = SPLIT && A.nparts > 1;
@@ -495,19 +562,19 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int ti
         Walk<D, 0, P, SPLIT>::run(A, sx, tid, A.nm1, cur, rg, in, xC, xA, xB, pin, ix, sum, comp);
     } else {
         uint32_t base[P];
-        float s[P];
+        FV<P> s;
 #pragma unroll
         for (int p = 0; p < P; ++p) base[p] = 0;
         block_sum<D, P>(A, A.nm1, in, xC, xA, xB, base, s);
-#pragma unroll
-        for (int p = 0; p < P; ++p) kahan_add(sum[p], comp[p], s[p]);
+        kahan_add(sum, comp, s);
     }
 
+    const FV<P> res = vsub(sum, comp);
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         const int64_t i = first + 32 * p;
         if (i < end) {
-            const float r = valid[p] ? __fsub_rn(sum[p], comp[p]) : (nan_in[p] ? __int_as_float(0x7fc00000) : 0.0f);
+            const float r = valid[p] ? res.get(p) : (nan_in[p] ? __int_as_float(0x7fc00000) : 0.0f);
             if (SPLIT && A.nparts > 1)
                 A.part_out[(int64_t)part * A.num_evals + i] = r;
             else
@@ -516,14 +583,20 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, int ti
     }
 }
 
+/* Dynamic shared memory of one CTA: the hats of dims A and C (kHatSlots
+ * FV<P> per thread), then the prefix coordinates (NPX * P floats per thread). */
+template <int D, int P>
+constexpr int kSmemBytes = kHatSlots * kThreads * (int)sizeof(FV<P>) + (D >= 4 ? D - 3 : 1) * P * kThreads * 4;
+
 template <int D, int P>
 __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const EvalArgs A)
 {
-    constexpr int NPX = D >= 4 ? D - 3 : 1; /* prefix coordinates kept in shared memory */
-    __shared__ float sx[NPX * P * kThreads];
+    extern __shared__ __align__(16) unsigned char smem_ev[];
+    FV<P> *shat = reinterpret_cast<FV<P> *>(smem_ev);
+    float *sx = reinterpret_cast<float *>(smem_ev + kHatSlots * kThreads * sizeof(FV<P>));
     const int tid = threadIdx.x;
     const int64_t warp = (blockIdx.x * (int64_t)kThreads + tid) >> 5;
-    eval_points<D, P, false>(A, sx, tid, warp * (32 * P) + (tid & 31), A.num_evals, 0);
+    eval_points<D, P, false>(A, sx, shat, tid, warp * (32 * P) + (tid & 31), A.num_evals, 0);
 }
 
 /* Many grids of the same dimension in one launch: CTA b evaluates the
@@ -533,12 +606,13 @@ template <int D, int P>
 __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3))
     k_evaluate_batch(const EvalArgs *__restrict__ grids, const int2 *__restrict__ items)
 {
-    constexpr int NPX = D >= 4 ? D - 3 : 1;
-    __shared__ float sx[NPX * P * kThreads];
+    extern __shared__ __align__(16) unsigned char smem_ev[];
+    FV<P> *shat = reinterpret_cast<FV<P> *>(smem_ev);
+    float *sx = reinterpret_cast<float *>(smem_ev + kHatSlots * kThreads * sizeof(FV<P>));
     __shared__ EvalArgs sA;
     const int tid = threadIdx.x;
     const int2 item = items[blockIdx.x];
-    const int q = item.x & 0x1FFFFFFF, part = (int)((unsigned)item.x >> 29); /* grid, part of a split sum */
+    const int q = item.x & 0x1FFFFFFF, part = (int)((unsigned)item.x >> 29);
     {
         const uint32_t *src = reinterpret_cast<const uint32_t *>(grids + q);
         uint32_t *dst = reinterpret_cast<uint32_t *>(&sA);
@@ -547,7 +621,7 @@ __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3))
     __syncthreads();
     const int64_t start = item.y;
     const int64_t end = min(start + (int64_t)kThreads * P, sA.num_evals);
-    eval_points<D, P, true>(sA, sx, tid, start + (tid >> 5) * (32 * P) + (tid & 31), end, part);
+    eval_points<D, P, true>(sA, sx, shat, tid, start + (tid >> 5) * (32 * P) + (tid & 31), end, part);
 }
 
 template <int D, int P>
@@ -556,12 +630,29 @@ int launch_eval(const EvalArgs &A, void *stream)
     const int64_t per_block = (int64_t)kThreads * P;
     const int64_t blocks = (A.num_evals + per_block - 1) / per_block;
     if (blocks > 0x7fffffff) return cudaErrorInvalidValue;
-    k_evaluate<D, P><<<(unsigned)blocks, kThreads, 0, (cudaStream_t)stream>>>(A);
+    k_evaluate<D, P><<<(unsigned)blocks, kThreads, kSmemBytes<D, P>, (cudaStream_t)stream>>>(A);
     sgk_count(1);
     return cudaGetLastError();
 }
 
 } // namespace sgeval
+
+/* Lets the kernels of dimension D use their dynamic shared memory (above
+ * 48 KB for d >= 8 at two points per thread) on the current device; called
+ * once per device before the first launch (outside any stream capture). */
+template <int D>
+int eval_setup()
+{
+    int e = cudaFuncSetAttribute(sgeval::k_evaluate<D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 sgeval::kSmemBytes<D, 1>);
+    if (!e) e = cudaFuncSetAttribute(sgeval::k_evaluate<D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     sgeval::kSmemBytes<D, 2>);
+    if (!e) e = cudaFuncSetAttribute(sgeval::k_evaluate_batch<D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     sgeval::kSmemBytes<D, 1>);
+    if (!e) e = cudaFuncSetAttribute(sgeval::k_evaluate_batch<D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     sgeval::kSmemBytes<D, 2>);
+    return e;
+}
 
 template <int D>
 int eval_launch(const EvalArgs &A, int ppt, void *stream)
@@ -575,9 +666,11 @@ int eval_batch_launch(const EvalArgs *grids, const int2 *items, int nitems, int 
 {
     if (nitems <= 0) return cudaSuccess;
     if (ppt == 1)
-        sgeval::k_evaluate_batch<D, 1><<<nitems, sgeval::kThreads, 0, (cudaStream_t)stream>>>(grids, items);
+        sgeval::k_evaluate_batch<D, 1>
+            <<<nitems, sgeval::kThreads, sgeval::kSmemBytes<D, 1>, (cudaStream_t)stream>>>(grids, items);
     else
-        sgeval::k_evaluate_batch<D, 2><<<nitems, sgeval::kThreads, 0, (cudaStream_t)stream>>>(grids, items);
+        sgeval::k_evaluate_batch<D, 2>
+            <<<nitems, sgeval::kThreads, sgeval::kSmemBytes<D, 2>, (cudaStream_t)stream>>>(grids, items);
     sgk_count(1);
     return cudaGetLastError();
 }

@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include "eval_args.h"
 #include "sg_kernels.h"
 
@@ -253,6 +255,24 @@ void sgk_fill_eval_args(const sg_eval_plan *p, const float *coords, const int32_
     for (int k = 0; k <= SG_EVAL_MAX_PARTS; ++k) A->split[k] = k ? 0xFFFFFFFFu : 0u;
     A->part_out = NULL;
     A->walk = NULL;
+}
+
+int sgk_eval_setup(void)
+{
+    /* once per device: the attribute calls are host-side and must not run
+     * inside a stream capture, so they come before any evaluation launch */
+    static std::atomic<int> done[64];
+    int dev = 0, e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+    if (done[dev].load(std::memory_order_acquire)) return cudaSuccess;
+#define SG_D(DD) \
+    if ((e = eval_setup<DD>()) != cudaSuccess) return e;
+    SG_D(1) SG_D(2) SG_D(3) SG_D(4) SG_D(5) SG_D(6) SG_D(7) SG_D(8) SG_D(9) SG_D(10)
+    SG_D(11) SG_D(12) SG_D(13) SG_D(14) SG_D(15) SG_D(16) SG_D(17) SG_D(18) SG_D(19) SG_D(20)
+#undef SG_D
+    done[dev].store(1, std::memory_order_release);
+    return cudaSuccess;
 }
 
 int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,

@@ -103,6 +103,12 @@ typedef struct sg_eval_args {
 void sgk_fill_eval_args(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
                         int64_t num_evals, sg_eval_args *a);
 
+/* Prepares the evaluation kernels on the current device (their dynamic
+ * shared-memory limit); done once per device, before any evaluation launch
+ * or stream capture.  The device-state set-up of grids, batches and servers
+ * calls it. */
+int sgk_eval_setup(void);
+
 /* out[perm ? perm[i] : i] = interpolant at coords[i*d .. i*d+d-1]. */
 int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm, float *out,
                  int64_t num_evals, void *stream);

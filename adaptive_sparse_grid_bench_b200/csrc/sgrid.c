@@ -261,6 +261,7 @@ static int materialize(sg_grid *g, cudaStream_t st)
     int k, r;
     cudaError_t ce;
     if (g->dev >= 0) return SG_OK;
+    CU((cudaError_t)sgk_eval_setup(), "evaluation kernel set-up");
     CU(cudaGetDevice(&g->dev), "cudaGetDevice");
     if ((r = dev_alloc(g, (void **)&g->d_alpha, L->Npad * 4, "grid values")) != SG_OK) goto bad;
     if ((ce = cudaMemsetAsync(g->d_alpha, 0, (size_t)L->Npad * 4, st)) != cudaSuccess) {

@@ -269,6 +269,7 @@ static int materialize(sg_batch *b)
     memset(nsegB, 0, sizeof(nsegB));
     memset(capchB, 0, sizeof(capchB));
     memset(capsegB, 0, sizeof(capsegB));
+    BCU((cudaError_t)sgk_eval_setup(), "evaluation kernel set-up");
     BCU(cudaGetDevice(&b->dev), "cudaGetDevice");
     if ((r = balloc(b, (void **)&b->d_alpha, b->doff[b->ng] * 4, "batch values")) != SG_OK) goto done;
     BCU(cudaMemset(b->d_alpha, 0, (size_t)b->doff[b->ng] * 4), "cudaMemset");

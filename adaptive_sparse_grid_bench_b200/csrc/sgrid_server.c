@@ -593,7 +593,7 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
     *out = NULL;
     s = (sg_server *)calloc(1, sizeof(sg_server));
     if (!s) return sfail(SG_ERR_NOMEM, "sg_server_create: out of host memory");
-    if (cudaGetDevice(&s->dev) != cudaSuccess) {
+    if (cudaGetDevice(&s->dev) != cudaSuccess || sgk_eval_setup() != cudaSuccess) {
         free(s);
         return sfail(SG_ERR_CUDA, "sg_server_create: no CUDA device");
     }
