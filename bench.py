@@ -58,8 +58,8 @@ EVAL_SRC = os.path.join(ROOT, "adaptive_sparse_grid_bench_b200", "csrc", "eval_i
 #     2^24-point launch (one-pass metrics, so the full launch was captured);
 #   inst_per_pair: smsp__inst_executed.sum x 32 / (points x subspaces) of a
 #     262,144-point launch of the same grid.
-EVAL_CAPTURE = {"source_sha16": "1330356f2d1d44e3", "captured": "2026-12-04", "dram_bytes": 2.02e9 + 0.553e9,
-                "inst_per_pair": 12.9}
+EVAL_CAPTURE = {"source_sha16": "44f82de6e967df93", "captured": "2026-12-04", "dram_bytes": 2.032e9 + 0.556e9,
+                "inst_per_pair": 10.41}
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -272,8 +272,8 @@ def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsampl
                   wl=None):
     """Error of the GPU results against the FP64 oracle (FP64 hierarchize +
     evaluate of the same nodal values) on `nsample` query points spread over
-    the launch (checker only).  max_rel_floor1e-3 is the per-point relative
-    error |u - u64| / max(|u64|, 1e-3 max|u64|)."""
+    the launch (checker only).  max_rel_floor1e-2 is the per-point relative
+    error |u - u64| / max(|u64|, 1e-2 max|u64|), the tests' bound."""
     from oracle.oracle import Oracle
     wl = wl or single_workload()
     o = Oracle(wl["d"], wl["n"], wl["limits"])
@@ -282,9 +282,9 @@ def error_vs_fp64(values: np.ndarray, gpu_out: np.ndarray, X: np.ndarray, nsampl
     u64 = o.evaluate_f64(s64, X[idx])
     err = np.abs(gpu_out[idx].astype(np.float64) - u64)
     scale = float(np.max(np.abs(u64)))
-    floor = 1e-3 * scale
+    floor = 1e-2 * scale
     res = {"points": int(nsample), "max_abs": float(err.max()), "norm_rel": float(err.max() / scale),
-           "max_rel_floor1e-3": float(np.max(err / np.maximum(np.abs(u64), floor)))}
+           "max_rel_floor1e-2": float(np.max(err / np.maximum(np.abs(u64), floor)))}
     if ref_out is not None:
         e2 = np.abs(ref_out[idx[idx < ref_out.shape[0]]].astype(np.float64) - u64[idx < ref_out.shape[0]])
         if e2.size:
@@ -711,10 +711,10 @@ def batch_error_vs_fp64(b, nodal: np.ndarray, dims, levels, out: np.ndarray, xs:
             scale = max(float(np.max(np.abs(u64))), 1e-30)
             worst_abs = max(worst_abs, float(e.max()))
             worst_rel = max(worst_rel, float(e.max()) / scale)
-            worst_pt = max(worst_pt, float(np.max(e / np.maximum(np.abs(u64), 1e-3 * scale))))
+            worst_pt = max(worst_pt, float(np.max(e / np.maximum(np.abs(u64), 1e-2 * scale))))
             checked += 1
     return {"grids": checked, "points_per_grid": npts, "max_abs": worst_abs, "max_norm_rel": worst_rel,
-            "max_rel_floor1e-3": worst_pt,
+            "max_rel_floor1e-2": worst_pt,
             "note": "FP32 batched results vs FP64 hierarchize + evaluate of the same nodal values"}
 
 
@@ -739,9 +739,9 @@ def served_error_vs_fp64(served, gsrc, dims, levels, coef, npts: int = 256):
         scale = max(float(np.max(np.abs(u64))), 1e-30)
         worst_abs = max(worst_abs, float(e.max()))
         worst_norm = max(worst_norm, float(e.max()) / scale)
-        worst_pt = max(worst_pt, float(np.max(e / np.maximum(np.abs(u64), 1e-3 * scale))))
+        worst_pt = max(worst_pt, float(np.max(e / np.maximum(np.abs(u64), 1e-2 * scale))))
     return {"requests": len(served), "points_per_request": npts, "max_abs": worst_abs, "max_norm_rel": worst_norm,
-            "max_rel_floor1e-3": worst_pt}
+            "max_rel_floor1e-2": worst_pt}
 
 
 def run_served(args, rank: int, world: int, local_rank: int):
