@@ -48,8 +48,8 @@
 #include "sg_kernels.h"
 
 #define SG_API __attribute__((visibility("default")))
-#define SRV_SLOTS 4               /* slots 0-1: light lane, 2-3: heavy lane */
-#define SRV_LANE_SLOTS 2
+#define SRV_SLOTS 5               /* slots 0-2: light lane, 3-4: heavy lane */
+#define SRV_LIGHT_SLOTS 3
 #define SRV_HEAVY_PAIRS ((int64_t)1 << 27) /* default SG_SRV_OPT_HEAVY_PAIRS */
 #define SRV_MAX_REQS 8192 /* requests per batch */
 #define SRV_CTA_THREADS 256
@@ -234,6 +234,7 @@ struct sg_server {
     int64_t max_points;
     int zero_copy; /* SG_SRV_OPT_ZERO_COPY */
     int64_t heavy_pairs; /* SG_SRV_OPT_HEAVY_PAIRS */
+    int light_slots;     /* SG_SRV_OPT_LIGHT_SLOTS */
     /* staging ring (pinned, mapped): submit copies a request's coordinates
      * here in the caller's thread; allocations are freed in any order and
      * reclaimed from the oldest */
@@ -499,7 +500,8 @@ static void *dispatcher(void *arg)
         /* light lane first: its slots run at the higher stream priority */
         for (i = 0; i < SRV_SLOTS; i++) {
             if (s->slot[i].busy) any_busy = 1;
-            else if (free_slot < 0 && s->head[s->slot[i].lane]) free_slot = i;
+            else if (free_slot < 0 && s->head[s->slot[i].lane] && (s->slot[i].lane || i < s->light_slots))
+                free_slot = i;
         }
         if (free_slot >= 0 && !s->fatal) {
             srv_slot *sl = &s->slot[free_slot];
@@ -601,6 +603,7 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
     s->max_points = max_batch_points;
     s->zero_copy = 1;
     s->heavy_pairs = SRV_HEAVY_PAIRS;
+    s->light_slots = SRV_LIGHT_SLOTS;
     max_items = ((max_batch_points + SRV_CTA_THREADS - 1) / SRV_CTA_THREADS + SRV_MAX_REQS) * SG_EVAL_MAX_PARTS;
     pthread_mutex_init(&s->mu, NULL);
     pthread_mutex_init(&s->plain_mu, NULL);
@@ -617,8 +620,8 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
         /* light batches at the highest priority, heavy ones one step below
          * (still above admissions): as CTAs retire, light work takes SMs
          * before the remaining CTAs of a heavy batch */
-        const int prio = i < SRV_LANE_SLOTS ? prio_high : (prio_high < prio_low ? prio_high + 1 : prio_high);
-        sl->lane = i < SRV_LANE_SLOTS ? 0 : 1;
+        const int prio = i < SRV_LIGHT_SLOTS ? prio_high : (prio_high < prio_low ? prio_high + 1 : prio_high);
+        sl->lane = i < SRV_LIGHT_SLOTS ? 0 : 1;
         for (d = 1; d <= SG_MAX_DIMS && ok; d++)
             ok = cudaStreamCreateWithPriority(&sl->dst[d], cudaStreamNonBlocking, prio) == cudaSuccess &&
                  cudaEventCreateWithFlags(&sl->ev_d[d], cudaEventDisableTiming) == cudaSuccess;
@@ -941,6 +944,12 @@ SG_API int sg_server_set_option(sg_server *s, int option, int64_t value)
         if (value != 0 && value != 1) return sfail(SG_ERR_ARG, "SG_SRV_OPT_ZERO_COPY is 0 or 1");
         pthread_mutex_lock(&s->mu);
         s->zero_copy = (int)value;
+        pthread_mutex_unlock(&s->mu);
+        return SG_OK;
+    case SG_SRV_OPT_LIGHT_SLOTS:
+        if (value < 1 || value > SRV_LIGHT_SLOTS) return sfail(SG_ERR_ARG, "SG_SRV_OPT_LIGHT_SLOTS is 1 .. %d", SRV_LIGHT_SLOTS);
+        pthread_mutex_lock(&s->mu);
+        s->light_slots = (int)value;
         pthread_mutex_unlock(&s->mu);
         return SG_OK;
     case SG_SRV_OPT_HEAVY_PAIRS:

@@ -95,6 +95,8 @@ def parse():
                     help="served: SG_SRV_OPT_ZERO_COPY (batches read and write pinned host memory in place)")
     ap.add_argument("--heavy-pairs", type=int, default=None,
                     help="served: SG_SRV_OPT_HEAVY_PAIRS (requests with this much work take the heavy lane)")
+    ap.add_argument("--light-slots", type=int, default=None,
+                    help="served: SG_SRV_OPT_LIGHT_SLOTS (light-lane batches in flight at once)")
     ap.add_argument("--served-dump", default=None,
                     help="served: save each rate's per-request timeline (ms to batch, launch, completion, delivery; "
                          "points; pairs) to PREFIX_<rate>.npy")
@@ -771,6 +773,9 @@ def run_served(args, rank: int, world: int, local_rank: int):
     if args.heavy_pairs is not None:
         from adaptive_sparse_grid_bench_b200._lib import SG_SRV_OPT_HEAVY_PAIRS
         srv.set_option(SG_SRV_OPT_HEAVY_PAIRS, args.heavy_pairs)
+    if args.light_slots is not None:
+        from adaptive_sparse_grid_bench_b200._lib import SG_SRV_OPT_LIGHT_SLOTS
+        srv.set_option(SG_SRV_OPT_LIGHT_SLOTS, args.light_slots)
     t0 = time.perf_counter()
     ids = [srv.add_grid(int(d), int(n), SG_FN_QUAD, coef[g, :3 * d]) for g, (d, n) in enumerate(zip(dims, levels))]
     admit_s = time.perf_counter() - t0
@@ -928,7 +933,7 @@ def run_served(args, rank: int, world: int, local_rank: int):
                                f"{100 - 100 * args.create_frac:g}% evaluate (1..65536 log-uniform points), "
                                f"{100 * args.create_frac:g}% create+hierarchize", "cap_gb": args.cap_gb,
                    "requests_per_rate": args.requests, "batch_points": max(args.batch_points, 65536),
-                   "zero_copy": args.zero_copy, "heavy_pairs": args.heavy_pairs},
+                   "zero_copy": args.zero_copy, "heavy_pairs": args.heavy_pairs, "light_slots": args.light_slots},
         "sweep": sweep, "burst": burst,
         "best_rate_with_p99_le_2ms": best,
         "plain_per_request": {"evals_per_s": plain_rate, "requests": len(plain),

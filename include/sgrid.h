@@ -263,10 +263,10 @@ int sg_batch_device_bytes(const sg_batch *batch, int64_t *bytes);
  * cap, and a dispatcher thread that batches evaluate requests continuously.
  * Requests are queued in two lanes by their work (points x grid subspaces,
  * SG_SRV_OPT_HEAVY_PAIRS); every request of a lane queued when one of the
- * lane's two batch slots frees up goes into one batch (one batched launch
- * per dimension), so one batch is assembled while the other computes, and
- * light batches run at a higher stream priority than heavy ones.  No
- * reference counterpart. */
+ * lane's batch slots frees up goes into one batch (one batched launch per
+ * dimension), so batches are assembled while others compute, and light
+ * batches run at a higher stream priority than heavy ones.  No reference
+ * counterpart. */
 typedef struct sg_server sg_server;
 /* max_batch_points: points per batch (and the largest single request).
  * Reserves hbm_cap_bytes of device memory at once (SG_ERR_NOMEM if it is not
@@ -304,6 +304,8 @@ int sg_server_wait_detail(sg_server *server, int64_t ticket, double *ms);
                                     (default 2^27) queue in the heavy lane: its own
                                     batches and slots at a lower stream priority, so
                                     light requests never wait behind them */
+#define SG_SRV_OPT_LIGHT_SLOTS 3 /* batches of the light lane in flight at once, 1..3
+                                    (default 3); the heavy lane has two */
 int sg_server_set_option(sg_server *server, int option, int64_t value);
 /* stats[7]: batches, requests, points, evictions, resident grids, bytes of
  * the reserved range in use, failed requests */

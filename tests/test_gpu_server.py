@@ -220,13 +220,14 @@ def test_zero_copy_ring_wraps_and_matches(cuda):
     ref.close()
 
 
-@pytest.mark.parametrize("heavy_pairs", [1, 1 << 22, 1 << 62])
-def test_lanes_keep_results(cuda, heavy_pairs):
+@pytest.mark.parametrize("heavy_pairs,light_slots", [(1, 3), (1 << 22, 3), (1 << 22, 1), (1 << 62, 2)])
+def test_lanes_keep_results(cuda, heavy_pairs, light_slots):
     """Requests split between the light and heavy lanes by their work give
     the same results as the plain call, whichever lane they take (all heavy,
-    mixed, all light)."""
+    mixed, all light) and however many light batches run at once."""
     srv, ids = _server()
     srv.set_option(_lib.SG_SRV_OPT_HEAVY_PAIRS, heavy_pairs)
+    srv.set_option(_lib.SG_SRV_OPT_LIGHT_SLOTS, light_slots)
     tickets = []
     for q in range(48):
         g = (5 * q) % len(ids)
@@ -240,4 +241,6 @@ def test_lanes_keep_results(cuda, heavy_pairs):
                              d >= 4 and sg.Grid(d, n).num_subspaces >= SPLIT_SUBSPACES)
     with pytest.raises(sg.SgError):
         srv.set_option(_lib.SG_SRV_OPT_HEAVY_PAIRS, 0)
+    with pytest.raises(sg.SgError):
+        srv.set_option(_lib.SG_SRV_OPT_LIGHT_SLOTS, 4)
     srv.close()
