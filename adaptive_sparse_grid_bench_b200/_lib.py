@@ -36,6 +36,7 @@ SG_OPT_TEST_WAIT = 9
 SG_SRV_OPT_ZERO_COPY = 1
 SG_SRV_OPT_HEAVY_PAIRS = 2
 SG_SRV_OPT_LIGHT_SLOTS = 3
+SG_SRV_OPT_SORT_HEAVY = 4
 SG_NUM_PHASES = 3
 
 SG_FN_REFERENCE = 0

@@ -25,7 +25,9 @@ namespace {
 constexpr int kThreads = 256;
 
 /* Adds the parts of split sums in part order with Kahan compensation; CTA
- * b covers kThreads points of request items[b].x from point items[b].y. */
+ * b covers kThreads points of request items[b].x from point items[b].y
+ * (sorted positions when the request has a permutation: the sum of point i
+ * goes to out[perm[i]]). */
 __global__ void __launch_bounds__(kThreads) k_combine_parts(const sg_eval_args *__restrict__ grids,
                                                             const int2 *__restrict__ items)
 {
@@ -42,7 +44,7 @@ __global__ void __launch_bounds__(kThreads) k_combine_parts(const sg_eval_args *
         c = __fsub_rn(__fsub_rn(t, s), y);
         s = t;
     }
-    A->out[i] = __fsub_rn(s, c);
+    A->out[A->perm ? A->perm[i] : i] = __fsub_rn(s, c);
 }
 
 /* compact (group-aligned) layout -> block layout */

@@ -55,7 +55,9 @@
 #define SRV_CTA_THREADS 256
 #define SRV_SPLIT_SUBSPACES 4096  /* grids (d >= 4) with this many subspaces get split sums */
 #define SRV_PART_SUBSPACES 2048   /* about this many subspaces per part (at most 8 parts) */
-#define SRV_LONG_CHAIN 2048       /* launches with a part this long use 1 point per thread */
+#define SRV_LONG_CHAIN 2048       /* light launches with a part this long use 1 point per thread */
+#define SRV_WHOLE_POINTS 8192     /* heavy requests with this many points are not split: their
+                                     own points give the launch enough CTAs */
 #define SRV_RING_BATCHES 4        /* the staging ring holds this many full batches */
 
 #define ARENA_ALIGN 256
@@ -206,12 +208,17 @@ typedef struct srv_slot {
     int32_t *h_items, *d_items;   /* evaluation CTAs, grouped by dimension */
     int32_t *h_citems, *d_citems; /* combine CTAs of the split requests     */
     float *d_part;                /* parts of split sums                    */
+    float *d_sorted;              /* heavy slots: Morton-ordered coordinates */
+    int32_t *d_perm;              /* heavy slots: sorted position -> point  */
+    void *d_sscratch;             /* heavy slots: sort scratch              */
+    const float *sort_src[SRV_MAX_REQS]; /* heavy slots: each request's coordinates */
     srv_req *reqs[SRV_MAX_REQS];
     int64_t out_off[SRV_MAX_REQS], coord_off[SRV_MAX_REQS], part_off[SRV_MAX_REQS];
     int order[SRV_MAX_REQS];
     int nreq;
     double t_launch, t_gpu; /* launch_batch returned; completion seen */
     int zero_copy;          /* the server's setting when the batch was taken */
+    int sort;               /* the batch's requests are Morton-ordered first */
     int lane;               /* the queue this slot takes its batches from */
 } srv_slot;
 
@@ -235,6 +242,7 @@ struct sg_server {
     int zero_copy; /* SG_SRV_OPT_ZERO_COPY */
     int64_t heavy_pairs; /* SG_SRV_OPT_HEAVY_PAIRS */
     int light_slots;     /* SG_SRV_OPT_LIGHT_SLOTS */
+    int sort_heavy;      /* SG_SRV_OPT_SORT_HEAVY */
     /* staging ring (pinned, mapped): submit copies a request's coordinates
      * here in the caller's thread; allocations are freed in any order and
      * reclaimed from the oldest */
@@ -340,6 +348,12 @@ static void finish_slot(sg_server *s, srv_slot *sl, int ok)
     pthread_cond_broadcast(&s->cv_done);
 }
 
+/* A heavy request with many points is evaluated with whole sums (one CTA
+ * per 512 points gives it enough parallelism): split sums would only add
+ * the walk's range checks and the combine.  The choice depends on the
+ * request alone, so its result is the same in any batch. */
+static int whole_sums(const srv_req *r) { return r->lane == 1 && r->m >= SRV_WHOLE_POINTS; }
+
 /* Moves queued requests into slot sl (lock held): pointers and offsets
  * only; returns their count. */
 static int take_batch(sg_server *s, srv_slot *sl)
@@ -361,7 +375,7 @@ static int take_batch(sg_server *s, srv_slot *sl)
         sl->out_off[sl->nreq] = pts;
         sl->coord_off[sl->nreq] = coff;
         sl->part_off[sl->nreq] = poff;
-        if (r->g->nparts > 1) poff += r->m * r->g->nparts;
+        if (r->g->nparts > 1 && !whole_sums(r)) poff += r->m * r->g->nparts;
         coff += r->m * r->d;
         pts += r->m;
         sl->nreq++;
@@ -389,6 +403,7 @@ static int launch_batch(sg_server *s, srv_slot *sl)
     int i, d, e, no = 0;
     int first[SG_MAX_DIMS + 1], count[SG_MAX_DIMS + 1], ppt[SG_MAX_DIMS + 1];
     const int zc = sl->zero_copy; /* fixed for the batch when it was taken */
+    const int sort = sl->sort;    /* heavy lane: spatial ordering of each request's points */
     for (i = 0; i < sl->nreq; i++) {
         srv_req *r = sl->reqs[i];
         int64_t p;
@@ -399,7 +414,18 @@ static int launch_batch(sg_server *s, srv_slot *sl)
             memcpy(sl->h_coords + sl->coord_off[i], r->coords, (size_t)(r->m * r->d) * sizeof(float));
             dc = (zc ? sl->m_coords : sl->d_coords) + sl->coord_off[i];
         }
+        if (sort) {
+            /* evaluated from the request's own Morton-ordered copy; the
+             * kernels write each result through the permutation */
+            sl->sort_src[i] = dc;
+            dc = sl->d_sorted + sl->coord_off[i];
+        }
         sg_grid_eval_args(r->g, dc, (zc ? sl->m_out : sl->d_out) + sl->out_off[i], r->m, &sl->h_args[i]);
+        if (sort) sl->h_args[i].perm = sl->d_perm + sl->out_off[i];
+        if (whole_sums(r)) {
+            sl->h_args[i].nparts = 1;
+            sl->h_args[i].part_out = NULL;
+        }
         if (sl->h_args[i].nparts > 1) {
             sl->h_args[i].part_out = sl->d_part + sl->part_off[i];
             for (p = 0; p < r->m; p += SRV_CTA_THREADS) {
@@ -422,7 +448,7 @@ static int launch_batch(sg_server *s, srv_slot *sl)
                 if (c > chain) chain = c;
             }
         sort_by_subspaces(sl, lo, no);
-        ppt[d] = chain >= SRV_LONG_CHAIN ? 1 : 2;
+        ppt[d] = (sl->lane == 0 && chain >= SRV_LONG_CHAIN) ? 1 : 2;
         cta = (int64_t)SRV_CTA_THREADS * ppt[d];
         for (i = lo; i < no; i++) {
             const int q = sl->order[i], np = sl->h_args[q].nparts;
@@ -443,9 +469,16 @@ static int launch_batch(sg_server *s, srv_slot *sl)
                         sl->st) != cudaSuccess ||
         cudaMemcpyAsync(sl->d_items, sl->h_items, (size_t)ni * 8, cudaMemcpyHostToDevice, sl->st) != cudaSuccess ||
         (nc && cudaMemcpyAsync(sl->d_citems, sl->h_citems, (size_t)nc * 8, cudaMemcpyHostToDevice, sl->st) !=
-                   cudaSuccess) ||
-        cudaEventRecord(sl->ev_in, sl->st) != cudaSuccess)
+                   cudaSuccess))
         return SG_ERR_CUDA;
+    for (i = 0; sort && i < sl->nreq; i++) {
+        const srv_req *r = sl->reqs[i];
+        /* issued after the copy in, so copied coordinates are in place */
+        if (sgk_sort_points(sl->sort_src[i], r->m, r->d, sl->d_sscratch, sl->d_sorted + sl->coord_off[i],
+                            sl->d_perm + sl->out_off[i], sl->st) != cudaSuccess)
+            return SG_ERR_CUDA;
+    }
+    if (cudaEventRecord(sl->ev_in, sl->st) != cudaSuccess) return SG_ERR_CUDA;
     for (d = 1; d <= SG_MAX_DIMS; d++) {
         if (!count[d]) continue;
         if (cudaStreamWaitEvent(sl->dst[d], sl->ev_in, 0) != cudaSuccess) return SG_ERR_CUDA;
@@ -507,6 +540,7 @@ static void *dispatcher(void *arg)
             srv_slot *sl = &s->slot[free_slot];
             take_batch(s, sl);
             sl->zero_copy = s->zero_copy;
+            sl->sort = sl->lane == 1 && s->sort_heavy && sl->d_sorted != NULL;
             sl->busy = 1;
             s->st_batches++;
             s->st_requests += sl->nreq;
@@ -578,6 +612,9 @@ static void free_slots(sg_server *s)
         cudaFreeHost(sl->h_citems);
         cudaFree(sl->d_citems);
         cudaFree(sl->d_part);
+        cudaFree(sl->d_sorted);
+        cudaFree(sl->d_perm);
+        cudaFree(sl->d_sscratch);
         cudaFree(sl->d_coords);
         cudaFree(sl->d_out);
         cudaFree(sl->d_args);
@@ -604,6 +641,7 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
     s->zero_copy = 1;
     s->heavy_pairs = SRV_HEAVY_PAIRS;
     s->light_slots = SRV_LIGHT_SLOTS;
+    s->sort_heavy = 1;
     max_items = ((max_batch_points + SRV_CTA_THREADS - 1) / SRV_CTA_THREADS + SRV_MAX_REQS) * SG_EVAL_MAX_PARTS;
     pthread_mutex_init(&s->mu, NULL);
     pthread_mutex_init(&s->plain_mu, NULL);
@@ -639,7 +677,12 @@ SG_API int sg_server_create(int64_t hbm_cap_bytes, int64_t max_batch_points, sg_
             cudaMalloc((void **)&sl->d_args, SRV_MAX_REQS * sizeof(sg_eval_args)) != cudaSuccess ||
             cudaMalloc((void **)&sl->d_items, (size_t)max_items * 8) != cudaSuccess ||
             cudaHostGetDevicePointer((void **)&sl->m_coords, sl->h_coords, 0) != cudaSuccess ||
-            cudaHostGetDevicePointer((void **)&sl->m_out, sl->h_out, 0) != cudaSuccess) {
+            cudaHostGetDevicePointer((void **)&sl->m_out, sl->h_out, 0) != cudaSuccess ||
+            (sl->lane == 1 &&
+             (cudaMalloc((void **)&sl->d_sorted, cb) != cudaSuccess ||
+              cudaMalloc((void **)&sl->d_perm, ob) != cudaSuccess ||
+              cudaMalloc(&sl->d_sscratch, (size_t)sgk_sort_scratch_bytes(max_batch_points, SG_MAX_DIMS)) !=
+                  cudaSuccess))) {
             cudaGetLastError();
             free_slots(s);
             free(s);
@@ -950,6 +993,12 @@ SG_API int sg_server_set_option(sg_server *s, int option, int64_t value)
         if (value < 1 || value > SRV_LIGHT_SLOTS) return sfail(SG_ERR_ARG, "SG_SRV_OPT_LIGHT_SLOTS is 1 .. %d", SRV_LIGHT_SLOTS);
         pthread_mutex_lock(&s->mu);
         s->light_slots = (int)value;
+        pthread_mutex_unlock(&s->mu);
+        return SG_OK;
+    case SG_SRV_OPT_SORT_HEAVY:
+        if (value != 0 && value != 1) return sfail(SG_ERR_ARG, "SG_SRV_OPT_SORT_HEAVY is 0 or 1");
+        pthread_mutex_lock(&s->mu);
+        s->sort_heavy = (int)value;
         pthread_mutex_unlock(&s->mu);
         return SG_OK;
     case SG_SRV_OPT_HEAVY_PAIRS:

@@ -97,6 +97,8 @@ def parse():
                     help="served: SG_SRV_OPT_HEAVY_PAIRS (requests with this much work take the heavy lane)")
     ap.add_argument("--light-slots", type=int, default=None,
                     help="served: SG_SRV_OPT_LIGHT_SLOTS (light-lane batches in flight at once)")
+    ap.add_argument("--sort-heavy", type=int, default=None, choices=[0, 1],
+                    help="served: SG_SRV_OPT_SORT_HEAVY (spatial ordering of heavy requests' points)")
     ap.add_argument("--served-dump", default=None,
                     help="served: save each rate's per-request timeline (ms to batch, launch, completion, delivery; "
                          "points; pairs) to PREFIX_<rate>.npy")
@@ -565,6 +567,8 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None, extras: bool
         line["err_vs_fp64"] = error_vs_fp64(vals, out_d.cpu().numpy(), X, ref_out=info["ref_out"], wl=wl)
     elif world == 1 and err:
         line["err_vs_fp64"] = error_vs_fp64(vals_d.cpu().numpy(), out_d.cpu().numpy(), X, nsample=256, wl=wl)
+    if world == 1 and extras:
+        line["reference_gpu"] = reference_gpu(g, X, out_d.cpu().numpy())
     del X_d, out_d, vals_d
     g.close()
     return line
@@ -773,6 +777,9 @@ def run_served(args, rank: int, world: int, local_rank: int):
     if args.heavy_pairs is not None:
         from adaptive_sparse_grid_bench_b200._lib import SG_SRV_OPT_HEAVY_PAIRS
         srv.set_option(SG_SRV_OPT_HEAVY_PAIRS, args.heavy_pairs)
+    if args.sort_heavy is not None:
+        from adaptive_sparse_grid_bench_b200._lib import SG_SRV_OPT_SORT_HEAVY
+        srv.set_option(SG_SRV_OPT_SORT_HEAVY, args.sort_heavy)
     if args.light_slots is not None:
         from adaptive_sparse_grid_bench_b200._lib import SG_SRV_OPT_LIGHT_SLOTS
         srv.set_option(SG_SRV_OPT_LIGHT_SLOTS, args.light_slots)
@@ -933,7 +940,8 @@ def run_served(args, rank: int, world: int, local_rank: int):
                                f"{100 - 100 * args.create_frac:g}% evaluate (1..65536 log-uniform points), "
                                f"{100 * args.create_frac:g}% create+hierarchize", "cap_gb": args.cap_gb,
                    "requests_per_rate": args.requests, "batch_points": max(args.batch_points, 65536),
-                   "zero_copy": args.zero_copy, "heavy_pairs": args.heavy_pairs, "light_slots": args.light_slots},
+                   "zero_copy": args.zero_copy, "heavy_pairs": args.heavy_pairs, "light_slots": args.light_slots,
+                   "sort_heavy": args.sort_heavy},
         "sweep": sweep, "burst": burst,
         "best_rate_with_p99_le_2ms": best,
         "plain_per_request": {"evals_per_s": plain_rate, "requests": len(plain),
@@ -964,6 +972,33 @@ def launch_ranks(n: int, argv) -> int:
 
 def compact(line: dict | None, keys) -> dict | None:
     return None if line is None else {k: line[k] for k in keys if k in line}
+
+
+def reference_gpu(g, X: np.ndarray, ours: np.ndarray, m: int = 1 << 18) -> dict:
+    """The reference's own CUDA evaluation kernel (evaluate5, cu:1522-1598,
+    compiled in place by oracle/ref_cuda_harness.cu) on the same hierarchized
+    grid and the first m query points, points per warp swept over the values
+    its run script uses (run.sh:14-18).  kernel: its kernel alone; copies: its
+    own timed region (coordinates in, kernel, results out, cu:1829-1897)."""
+    from oracle.oracle import ReferenceCUDA
+    if not ReferenceCUDA.available():
+        return {"unavailable": "oracle/_ref/libasgb_refcuda.so not built"}
+    surplus = g.get_values()
+    Xm = np.ascontiguousarray(X[:m])
+    sweep, best = {}, None
+    for P in (32, 64, 128, 256):
+        out, tk, tt = ReferenceCUDA.evaluate5(g.d, g.n, surplus, Xm, P, reps=2)
+        sweep[P] = tk
+        if best is None or tk < best[1]:
+            best = (P, tk, tt, out)
+    P, tk, tt, out = best
+    scale = float(np.max(np.abs(ours[:m])))
+    return {"kernel": "reference evaluate5 (cu:1522-1598)", "points": m, "points_per_warp": P,
+            "kernel_ms": tk, "copies_ms": tt, "evals_per_s_kernel": m / (tk / 1e3),
+            "evals_per_s_copies": m / (tt / 1e3), "pairs_per_s_kernel": m * g.num_subspaces / (tk / 1e3),
+            "kernel_ms_by_points_per_warp": sweep,
+            "max_abs_diff_vs_b200": float(np.max(np.abs(out.astype(np.float64) - ours[:m]))),
+            "max_abs_b200": scale}
 
 
 def run_extras(args, rank: int, world: int, local_rank: int) -> dict:

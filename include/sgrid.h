@@ -306,6 +306,9 @@ int sg_server_wait_detail(sg_server *server, int64_t ticket, double *ms);
                                     light requests never wait behind them */
 #define SG_SRV_OPT_LIGHT_SLOTS 3 /* batches of the light lane in flight at once, 1..3
                                     (default 3); the heavy lane has two */
+#define SG_SRV_OPT_SORT_HEAVY 4  /* 1 (default): the points of each heavy request are
+                                    put in spatial (Morton) order on the GPU before
+                                    evaluation (results scattered back; same values) */
 int sg_server_set_option(sg_server *server, int option, int64_t value);
 /* stats[7]: batches, requests, points, evictions, resident grids, bytes of
  * the reserved range in use, failed requests */

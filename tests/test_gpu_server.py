@@ -220,14 +220,18 @@ def test_zero_copy_ring_wraps_and_matches(cuda):
     ref.close()
 
 
-@pytest.mark.parametrize("heavy_pairs,light_slots", [(1, 3), (1 << 22, 3), (1 << 22, 1), (1 << 62, 2)])
-def test_lanes_keep_results(cuda, heavy_pairs, light_slots):
+@pytest.mark.parametrize("heavy_pairs,light_slots,sort,zero_copy",
+                         [(1, 3, 1, 1), (1, 3, 0, 1), (1, 2, 1, 0), (1 << 22, 3, 1, 1), (1 << 22, 1, 1, 1),
+                          (1 << 62, 2, 1, 1)])
+def test_lanes_keep_results(cuda, heavy_pairs, light_slots, sort, zero_copy):
     """Requests split between the light and heavy lanes by their work give
     the same results as the plain call, whichever lane they take (all heavy,
-    mixed, all light) and however many light batches run at once."""
-    srv, ids = _server()
+    mixed, all light), however many light batches run at once, with the
+    heavy requests' points spatially ordered or not, zero-copy or copied."""
+    srv, ids = _server(zero_copy=zero_copy)
     srv.set_option(_lib.SG_SRV_OPT_HEAVY_PAIRS, heavy_pairs)
     srv.set_option(_lib.SG_SRV_OPT_LIGHT_SLOTS, light_slots)
+    srv.set_option(_lib.SG_SRV_OPT_SORT_HEAVY, sort)
     tickets = []
     for q in range(48):
         g = (5 * q) % len(ids)
@@ -243,4 +247,6 @@ def test_lanes_keep_results(cuda, heavy_pairs, light_slots):
         srv.set_option(_lib.SG_SRV_OPT_HEAVY_PAIRS, 0)
     with pytest.raises(sg.SgError):
         srv.set_option(_lib.SG_SRV_OPT_LIGHT_SLOTS, 4)
+    with pytest.raises(sg.SgError):
+        srv.set_option(_lib.SG_SRV_OPT_SORT_HEAVY, 2)
     srv.close()
