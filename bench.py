@@ -85,7 +85,8 @@ def parse():
     ap.add_argument("--no-graph", action="store_true",
                     help="batched: launch kernels directly instead of replaying CUDA graphs (for profilers that "
                          "cannot follow stream capture)")
-    ap.add_argument("--rates", default="1000,2000,4000,8000,16000", help="served: arrival rates (requests/s)")
+    ap.add_argument("--rates", default="4000,8000,16000,20000,24000,28000",
+                    help="served: arrival rates (requests/s)")
     ap.add_argument("--requests", type=int, default=3000, help="served: requests per rate")
     ap.add_argument("--cap-gb", type=float, default=60.0, help="served: resident-grid byte cap")
     ap.add_argument("--create-frac", type=float, default=0.05, help="served: share of create+hierarchize requests")
@@ -1003,7 +1004,7 @@ def reference_gpu(g, X: np.ndarray, ours: np.ndarray, m: int = 1 << 18) -> dict:
 
 def run_extras(args, rank: int, world: int, local_rank: int) -> dict:
     """Short runs of the other workloads for the N=1 default line: the
-    batched step on 1024 grids, the served sweep at three rates with 1000
+    batched step on 1024 grids, the served sweep at four rates with 3000
     requests each, and the limits-adaptive grid; each with its error against
     the FP64 oracle."""
     import copy
@@ -1015,7 +1016,7 @@ def run_extras(args, rank: int, world: int, local_rank: int) -> dict:
                              ["value", "unit", "ms_per_step", "config", "hierarchize", "evaluate", "plain_per_grid",
                               "speedup_vs_plain", "err_vs_fp64", "gpu_launches"])
     a = copy.copy(args)
-    a.rates, a.requests = "2000,4000,8000", 1000
+    a.rates, a.requests = "16000,20000,24000,28000", 3000
     srv = run_served(a, rank, world, local_rank)
     if srv is not None:
         srv = compact(srv, ["value", "unit", "sweep", "burst", "best_rate_with_p99_le_2ms", "plain_per_request",
