@@ -14,14 +14,15 @@
  * shared by all subspaces below a node.  Below a prefix cell the walk reads
  * one block: every subspace of the three innermost dims (C = d-3, A = d-2,
  * B = d-1), stored contiguously in the block layout (sg_layout.h) with dim
- * B's levels as a 1-D heap.  The surplus of (c, a, b) sits at
- *     base + coff(c) + t_c sub(R-c) + aoff(a) + t_a plen(a) + (2^b - 1 + t_b):
+ * B's levels as paths: per finest cell t_L of a row, the L+1 surpluses a
+ * point in that cell needs, side by side.  The surplus of (c, a, b) sits at
+ *     base + coff(c) + t_c sub(R-c) + aoff(a) + t_a plen(a) + t_L (L+1) + b:
  *   - blocks follow each other in walk order, so the block base is a running
  *     counter plus one multiply-add per point (no table);
- *   - 2^b - 1 + t_b and the hats of dim B are precomputed per point in
- *     registers, the hats of dims A and C in this thread's column of shared
- *     memory (registers held them before: 128 registers with spills), so
- *     each subspace costs one add, one gather and one FMA;
+ *   - a row's L+1 loads share one address (the point's path) and differ by
+ *     a constant, so each subspace costs one gather and one FMA, the row one
+ *     address; the hats of dim B are precomputed per point in registers,
+ *     those of dims A and C in this thread's column of shared memory;
  *   - the two points of a thread are computed with Blackwell's packed FP32x2
  *     instructions (FFMA2, FADD2, FMUL2 through __ffma2_rn, __fadd2_rn,
  *     __fmul2_rn): one instruction does both points' FMA, product or
@@ -132,7 +133,7 @@ __device__ __forceinline__ FV<P> hats(const FV<P> &y)
 template <int P>
 struct Inner {
     FV<P> hB[kNB];        /* hat of dim B at level b                 */
-    uint32_t cB[P][kNB];  /* heap index 2^b - 1 + t_b of dim B       */
+    uint32_t TB[P];       /* floor(x_B 2^15): the path t_L = TB >> (15 - L) */
     const FV<P> *sh;      /* this thread's hats of dims A, C in smem */
     uint32_t TA[P];       /* floor(x_A 2^15): t_a = TA >> (15 - a)   */
     uint32_t TC[P];       /* floor(x_C 2^15)                         */
@@ -142,7 +143,7 @@ struct Inner {
 constexpr int kHatSlots = kNB + kRF + 1;
 
 /* Regular shapes: blocks whose budget is within the innermost limits. */
-__host__ __device__ constexpr uint32_t plen_reg(int r, int a) { return (2u << (r - a)) - 1u; }
+__host__ __device__ constexpr uint32_t plen_reg(int r, int a) { return (1u << (r - a)) * (uint32_t)(r - a + 1); }
 __host__ __device__ constexpr uint32_t aoff_reg(int r, int a)
 {
     uint32_t o = 0;
@@ -165,15 +166,18 @@ __device__ __forceinline__ void block2_fixed(const float *__restrict__ alpha, co
 {
 #pragma unroll
     for (int a = 0; a <= r; ++a) {
-        uint32_t rb[P];
+        const int L = r - a; /* compile-time after unrolling */
+        const float *path[P]; /* the point's path: its L+1 surpluses of this row */
 #pragma unroll
-        for (int p = 0; p < P; ++p) rb[p] = base[p] + aoff_reg(r, a) + (in.TA[p] >> (kTB - a)) * plen_reg(r, a);
+        for (int p = 0; p < P; ++p)
+            path[p] = alpha + (base[p] + aoff_reg(r, a) + (in.TA[p] >> (kTB - a)) * plen_reg(r, a) +
+                               (in.TB[p] >> (kTB - L)) * (uint32_t)(L + 1));
         FV<P> sr = FV<P>::all(0.0f);
 #pragma unroll
-        for (int b = 0; b <= r - a; ++b) {
+        for (int b = 0; b <= L; ++b) {
             FV<P> v;
 #pragma unroll
-            for (int p = 0; p < P; ++p) v.set(p, __ldg(alpha + rb[p] + in.cB[p][b]));
+            for (int p = 0; p < P; ++p) v.set(p, __ldg(path[p] + b));
             sr = vfma(in.hB[b], v, sr);
         }
         s = (a == 0) ? vmul(in.hA(0), sr) : vfma(in.hA(a), sr, s);
@@ -220,27 +224,27 @@ __device__ __forceinline__ void block2_generic(const float *__restrict__ alpha, 
             }
         }
         const int rl = min(r - a, limB) + 1;
-        const uint32_t plen = (1u << rl) - 1u;
+        const uint32_t plen = (1u << (rl - 1)) * (uint32_t)rl;
         FV<P> yB, sr = FV<P>::all(0.0f);
-        uint32_t tB[P], rb[P];
+        uint32_t rb[P];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             yB.set(p, xB[p]);
-            tB[p] = 0;
-            rb[p] = base[p] + aoff + tA[p] * plen;
+            /* path of the finest cell t_L = floor(x_B 2^L), exact */
+            rb[p] = base[p] + aoff + tA[p] * plen + (uint32_t)(xB[p] * (float)(1u << (rl - 1))) * (uint32_t)rl;
         }
         for (int b = 0; b < rl; ++b) {
             if (b) {
 #pragma unroll
                 for (int p = 0; p < P; ++p) {
                     float y = yB.get(p);
-                    tB[p] = 2 * tB[p] + step_y(y);
+                    (void)step_y(y);
                     yB.set(p, y);
                 }
             }
             FV<P> v;
 #pragma unroll
-            for (int p = 0; p < P; ++p) v.set(p, __ldg(alpha + rb[p] + (1u << b) - 1u + tB[p]));
+            for (int p = 0; p < P; ++p) v.set(p, __ldg(alpha + rb[p] + b));
             sr = vfma(hats(yB), v, sr);
         }
         s = vfma(hasA ? hats(yA) : FV<P>::all(1.0f), sr, s);
@@ -314,6 +318,12 @@ __device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<
         coff += (1u << c) * sub;
     }
 }
+
+/* level state (y, cell index, parent product) of the upper prefix dims
+ * K < kUpper (K <= D-6, at most 7 of them so that two CTAs still fit an SM
+ * at d = 20), kept in shared memory while the subtree below runs */
+template <int D>
+constexpr int kUpper = D >= 6 ? (D - 5 < 7 ? D - 5 : 7) : 0;
 
 /* The walk's block range of a split evaluation: blocks are numbered in
  * walk order; only [lo, hi) are summed (all of them when !partial). */
@@ -398,6 +408,50 @@ struct Walk {
                                                const float (&xA)[P], const float (&xB)[P], const FV<P> &pin,
                                                const uint32_t (&ixin)[P], FV<P> &sum, FV<P> &comp)
     {
+        if constexpr (K + 6 <= D && K < kUpper<D>) {
+            /* upper prefix dim: its level state lives in this thread's
+             * shared-memory slots while the subtree below runs, so it holds
+             * no registers there */
+            constexpr int NPX = D >= 4 ? D - 3 : 1;
+            volatile float *ws = const_cast<float *>(sx) + NPX * P * kThreads + (K * 3 * P) * kThreads + tid;
+            const int lmax = min(A.lim[K], budget);
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                ws[(0 * P + p) * kThreads] = sx[(K * P + p) * kThreads + tid];
+                ws[(1 * P + p) * kThreads] = __uint_as_float(ixin[p]);
+                ws[(2 * P + p) * kThreads] = pin.get(p);
+            }
+            for (int l = 0; l <= lmax; ++l) {
+                FV<P> y, pp;
+                uint32_t ix[P];
+#pragma unroll
+                for (int p = 0; p < P; ++p) {
+                    y.set(p, ws[(0 * P + p) * kThreads]);
+                    ix[p] = __float_as_uint(ws[(1 * P + p) * kThreads]);
+                    pp.set(p, ws[(2 * P + p) * kThreads]);
+                }
+                if (l) {
+                    step_all<P>(y, ix);
+#pragma unroll
+                    for (int p = 0; p < P; ++p) {
+                        ws[(0 * P + p) * kThreads] = y.get(p);
+                        ws[(1 * P + p) * kThreads] = __uint_as_float(ix[p]);
+                    }
+                }
+                if (SPLIT && rg.partial) {
+                    const uint32_t *w = A.walk + 2 * ((K + 1) * (A.nm1 + 1) + (budget - l));
+                    const uint32_t nb = __ldg(w);
+                    if (rg.leaf + nb <= rg.lo || rg.leaf >= rg.hi) {
+                        rg.leaf += nb;
+                        cur += __ldg(w + 1);
+                        continue;
+                    }
+                }
+                const FV<P> pn = vmul(pp, hats(y));
+                Walk<D, K + 1, P, SPLIT>::run(A, sx, tid, budget - l, cur, rg, in, xC, xA, xB, pn, ix, sum, comp);
+            }
+            return;
+        }
         const int lmax = min(A.lim[K], budget);
         FV<P> y = load_y<P>(sx, K, tid);
         FV<P> acc = FV<P>::all(0.0f);
@@ -506,13 +560,12 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, FV<P> 
 #pragma unroll
     for (int p = 0; p < P; ++p) {
         float y = xB[p];
-        uint32_t t = 0;
 #pragma unroll
         for (int j = 0; j < kNB; ++j) {
-            if (j) t = 2 * t + step_y(y);
+            if (j) (void)step_y(y);
             in.hB[j].set(p, hat_of(y));
-            in.cB[p][j] = ((1u << j) - 1u) + t;
         }
+        in.TB[p] = (uint32_t)(xB[p] * (float)(1u << kTB));
         in.TA[p] = (uint32_t)(xA[p] * (float)(1u << kTB));
         in.TC[p] = (uint32_t)(xC[p] * (float)(1u << kTB));
     }
@@ -586,7 +639,8 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, FV<P> 
 /* Dynamic shared memory of one CTA: the hats of dims A and C (kHatSlots
  * FV<P> per thread), then the prefix coordinates (NPX * P floats per thread). */
 template <int D, int P>
-constexpr int kSmemBytes = kHatSlots * kThreads * (int)sizeof(FV<P>) + (D >= 4 ? D - 3 : 1) * P * kThreads * 4;
+constexpr int kSmemBytes = kHatSlots * kThreads * (int)sizeof(FV<P>) + (D >= 4 ? D - 3 : 1) * P * kThreads * 4 +
+                           kUpper<D> * 3 * P * kThreads * 4;
 
 template <int D, int P>
 __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const EvalArgs A)

@@ -47,7 +47,9 @@ __global__ void __launch_bounds__(kThreads) k_combine_parts(const sg_eval_args *
     A->out[A->perm ? A->perm[i] : i] = __fsub_rn(s, c);
 }
 
-/* compact (group-aligned) layout -> block layout */
+/* compact (group-aligned) layout -> block layout: every value of level b
+ * of dim B goes to slot b of the 2^(L-b) paths of its pole that pass
+ * through its cell */
 __global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
                          const sg_repack *__restrict__ rp, int64_t nsub)
 {
@@ -56,14 +58,18 @@ __global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
     const int64_t nw = (int64_t)gridDim.x * (blockDim.x >> 5);
     for (int64_t q = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); q < nsub; q += nw) {
         const sg_repack r = rp[q];
-        const int n = 1 << r.s;
         const int ab = r.a + r.b, cab = r.c + ab;
-        for (int e = threadIdx.x & 31; e < n; e += 32) {
-            const uint32_t I = (uint32_t)e >> cab;
-            const uint32_t tc = ((uint32_t)e >> ab) & ((1u << r.c) - 1u);
-            const uint32_t ta = ((uint32_t)e >> r.b) & ((1u << r.a) - 1u);
-            const uint32_t tb = (uint32_t)e & ((1u << r.b) - 1u);
-            dst[r.dst + I * r.blk + tc * r.sub + ta * r.plen + tb] = src[r.src + e];
+        const int rep = r.L - r.b; /* the value fills slot b of 2^rep paths */
+        const int n = 1 << (r.s + rep);
+        const uint32_t w = (uint32_t)r.L + 1u;
+        for (int f = threadIdx.x & 31; f < n; f += 32) {
+            const uint32_t e = (uint32_t)f >> rep, j = (uint32_t)f & ((1u << rep) - 1u);
+            const uint32_t I = e >> cab;
+            const uint32_t tc = (e >> ab) & ((1u << r.c) - 1u);
+            const uint32_t ta = (e >> r.b) & ((1u << r.a) - 1u);
+            const uint32_t tb = e & ((1u << r.b) - 1u);
+            const uint32_t path = (tb << rep) | j; /* finest cell t_L of the path */
+            dst[r.dst + I * r.blk + tc * r.sub + ta * r.plen + path * w] = src[r.src + e];
         }
     }
 }

@@ -10,6 +10,8 @@
 #include <stdlib.h>
 #include <string.h>
 
+static int64_t block_layout_size(const sg_layout *L);
+
 int sg_layout_init(sg_layout *L, int d, int n, const int *limits)
 {
     int i, s, k;
@@ -45,6 +47,8 @@ int sg_layout_init(sg_layout *L, int d, int n, const int *limits)
     L->plidx[n] = L->Npad;
     /* kernels index the device grid with 32-bit offsets */
     if (L->Npad >= ((int64_t)1 << 31)) return SG_ERR_RANGE;
+    L->Nblk = block_layout_size(L);
+    if (L->Nblk >= ((int64_t)1 << 32) - 64) return SG_ERR_RANGE;
     return SG_OK;
 }
 
@@ -225,7 +229,8 @@ void sg_layout_eval_sub(const sg_layout *L, int r, sg_eval_sub *sh)
         int rl = r - a < limB ? r - a : limB;
         sh->rowlen[a] = rl + 1;
         sh->aoff[a] = off;
-        off += ((uint32_t)1 << a) * (((uint32_t)1 << (rl + 1)) - 1);
+        /* 2^a poles of 2^rl paths of rl+1 slots */
+        off += ((uint32_t)1 << a) * (((uint32_t)1 << rl) * (uint32_t)(rl + 1));
     }
     sh->aoff[sh->amax + 1] = off;
 }
@@ -245,6 +250,28 @@ void sg_layout_eval_shape(const sg_layout *L, int R, sg_eval_shape *sh)
         off += ((uint32_t)1 << c) * sub.aoff[sub.amax + 1];
     }
     sh->coff[sh->cmax + 1] = off;
+}
+
+/* Values of the block layout: every prefix level vector's cells times the
+ * block size of its remaining budget. */
+static int64_t block_layout_size(const sg_layout *L)
+{
+    const int np_dims = L->d >= 3 ? L->d - 3 : 0;
+    int64_t sz[SG_MAX_DIMS + 1][SG_MAX_LEVELS];
+    int k, R;
+    for (R = 0; R < L->n; R++) {
+        sg_eval_shape sh;
+        sg_layout_eval_shape(L, R, &sh);
+        sz[np_dims][R] = sh.coff[sh.cmax + 1];
+    }
+    for (k = np_dims - 1; k >= 0; k--)
+        for (R = 0; R < L->n; R++) {
+            int l;
+            int64_t w = 0;
+            for (l = 0; l <= R && l <= L->lim[k]; l++) w += sz[k + 1][R - l] << l;
+            sz[k][R] = w;
+        }
+    return sz[0][L->n - 1];
 }
 
 int sg_layout_eval_tables(const sg_layout *L, sg_repack **repack, uint32_t *blk3, uint32_t *blk2)
@@ -278,7 +305,7 @@ int sg_layout_eval_tables(const sg_layout *L, sg_repack **repack, uint32_t *blk3
             cnt[k][R] = v;
             sz[k][R] = w;
         }
-    if (sz[0][L->n - 1] != L->N) return SG_ERR_STATE;
+    if (sz[0][L->n - 1] != L->Nblk) return SG_ERR_STATE;
     rp = (sg_repack *)malloc((size_t)(L->S > 0 ? L->S : 1) * sizeof(sg_repack));
     if (!rp) return SG_ERR_NOMEM;
     memset(lv, 0, sizeof(lv));
@@ -304,10 +331,12 @@ int sg_layout_eval_tables(const sg_layout *L, sg_repack **repack, uint32_t *blk3
             sg_layout_eval_shape(L, L->n - 1 - sigma, &sh);
             sg_layout_eval_sub(L, L->n - 1 - sigma - c, &sub);
             rp[r].src = (uint32_t)(L->plidx[s] + (pos << s));
-            rp[r].dst = (uint32_t)base + sh.coff[c] + sub.aoff[a] + (((uint32_t)1 << b) - 1);
+            rp[r].dst = (uint32_t)base + sh.coff[c] + sub.aoff[a] + (uint32_t)b;
             rp[r].blk = sh.coff[sh.cmax + 1];
             rp[r].sub = sub.aoff[sub.amax + 1];
-            rp[r].plen = ((uint32_t)1 << sub.rowlen[a]) - 1;
+            rp[r].plen = ((uint32_t)1 << (sub.rowlen[a] - 1)) * (uint32_t)sub.rowlen[a];
+            rp[r].L = (uint8_t)(sub.rowlen[a] - 1);
+            rp[r].pad[0] = rp[r].pad[1] = rp[r].pad[2] = 0;
             rp[r].c = (uint8_t)c;
             rp[r].a = (uint8_t)a;
             rp[r].b = (uint8_t)b;

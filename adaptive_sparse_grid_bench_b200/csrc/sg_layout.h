@@ -30,6 +30,7 @@ typedef struct sg_layout {
     int64_t lidx[SG_MAX_LEVELS + 1];        /* compact group offsets        */
     int64_t plidx[SG_MAX_LEVELS + 1];       /* device (padded) group offsets */
     int64_t N, S, Npad;
+    int64_t Nblk; /* values of the evaluation (block) layout */
 } sg_layout;
 
 /* One 1-D "chain" of sweep k: the subspaces that differ only in l_k.  They
@@ -68,10 +69,13 @@ int sg_layout_chains(const sg_layout *L, int k, sg_chain **chains, int64_t *ncha
  *   planes c = 0..cmax, each 2^c sub-blocks (one per cell t_c of dim C);
  *   a sub-block of budget r = R-c has rows a = 0..amax(r), each 2^a poles
  *   (one per cell t_a of dim A);
- *   a pole is the 1-D heap of dim B's levels b = 0..rowlen-1: cell t_b of
- *   level b sits at 2^b - 1 + t_b.
+ *   a pole holds dim B's levels b = 0..L (L = rowlen-1) as 2^L paths, one
+ *   per finest cell t_L: path t_L is the L+1 surpluses a query point in that
+ *   cell needs, level b's cell t_L >> (L-b) in slot b.  A surplus of level
+ *   b therefore appears in 2^(L-b) paths (Nblk >= N values in all).
  * A query point finds the surplus of (c, a, b) at
- *   base + coff(c) + t_c * sub(R-c) + aoff(R-c, a) + t_a * plen + 2^b - 1 + t_b.
+ *   base + coff(c) + t_c * sub(R-c) + aoff(R-c, a) + t_a * plen + t_L * (L+1) + b,
+ * so the L+1 loads of a row share one address and differ by a constant.
  */
 typedef struct sg_eval_sub {
     int amax;                         /* last row: min(r, lim_A)           */
@@ -100,11 +104,13 @@ int sg_layout_walk_split(const sg_layout *L, int nparts, uint32_t *bounds);
 /* Per-subspace repack descriptor (compact layout -> block layout). */
 typedef struct sg_repack {
     uint32_t src;  /* device offset of the subspace in the group-aligned layout */
-    uint32_t dst;  /* block-layout offset of its element with I = t = 0         */
+    uint32_t dst;  /* block-layout offset of its element with I = t = 0 (slot b) */
     uint32_t blk;  /* block size: stride of the prefix cell I                   */
     uint32_t sub;  /* sub-block size: stride of t_c                             */
     uint32_t plen; /* pole length: stride of t_a                                */
     uint8_t c, a, b, s;
+    uint8_t L;     /* last level of dim B in the row: paths of L+1 slots        */
+    uint8_t pad[3];
 } sg_repack;
 
 /* The repack table (one entry per subspace, malloc'd) and the block sizes

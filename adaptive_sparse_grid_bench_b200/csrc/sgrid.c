@@ -277,7 +277,7 @@ static int materialize(sg_grid *g, cudaStream_t st)
         fail(r, "building the evaluation layout tables");
         goto bad;
     }
-    if ((r = dev_alloc(g, (void **)&g->d_blk, L->N * 4, "block layout")) != SG_OK) goto bad;
+    if ((r = dev_alloc(g, (void **)&g->d_blk, L->Nblk * 4, "block layout")) != SG_OK) goto bad;
     if ((r = dev_alloc(g, (void **)&g->d_repack, L->S * (int64_t)sizeof(sg_repack), "repack table")) != SG_OK)
         goto bad;
     /* pageable sources: the copy has taken the bytes when the call returns */

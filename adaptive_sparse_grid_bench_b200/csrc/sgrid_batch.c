@@ -57,7 +57,7 @@ SG_API int sg_batch_create(int num_grids, const int *dims, const int *levels, co
 {
     sg_batch *b;
     int g, r;
-    int64_t lim_at = 0, doff = 0, voff = 0;
+    int64_t lim_at = 0, doff = 0, voff = 0, boff = 0;
     if (!out || num_grids < 1 || num_grids >= (1 << 29) || !dims || !levels)
         return bfail(SG_ERR_ARG, "sg_batch_create: bad argument");
     *out = NULL;
@@ -81,13 +81,19 @@ SG_API int sg_batch_create(int num_grids, const int *dims, const int *levels, co
         lim_at += dims[g];
         b->voff[g] = voff;
         b->doff[g] = doff;
-        b->boff[g] = voff;
+        b->boff[g] = boff;
         voff += b->L[g].N;
         doff += b->L[g].Npad;
+        boff += b->L[g].Nblk;
     }
     b->voff[num_grids] = voff;
     b->doff[num_grids] = doff;
-    b->boff[num_grids] = voff;
+    b->boff[num_grids] = boff;
+    if (boff >= ((int64_t)1 << 32) - 64) {
+        sg_batch_destroy(b);
+        return bfail(SG_ERR_RANGE, "sg_batch_create: %lld evaluation-layout values exceed 32-bit offsets",
+                     (long long)boff);
+    }
     if (doff >= ((int64_t)1 << 32) - 64) {
         sg_batch_destroy(b);
         return bfail(SG_ERR_RANGE, "sg_batch_create: %lld values exceed 32-bit offsets", (long long)doff);

@@ -776,7 +776,7 @@ SG_API int sg_server_destroy(sg_server *s)
  * tables), from its host layout */
 static int64_t grid_bytes_estimate(const sg_layout *L)
 {
-    return L->Npad * 4 + L->N * 4 + L->S * (int64_t)(sizeof(sg_repack) + 12 * L->d) + (1 << 16);
+    return L->Npad * 4 + L->Nblk * 4 + L->S * (int64_t)(sizeof(sg_repack) + 12 * L->d) + (1 << 16);
 }
 
 /* Evicts the least recently used grid that no request needs (lock held);
