@@ -143,7 +143,7 @@ struct Inner {
 constexpr int kHatSlots = kNB + kRF + 1;
 
 /* Regular shapes: blocks whose budget is within the innermost limits. */
-__host__ __device__ constexpr uint32_t plen_reg(int r, int a) { return (1u << (r - a)) * (uint32_t)(r - a + 1); }
+__host__ __device__ constexpr uint32_t plen_reg(int r, int a) { return (1u << (r - a)) * (uint32_t)SG_PATH_WIDTH(r - a + 1); }
 __host__ __device__ constexpr uint32_t aoff_reg(int r, int a)
 {
     uint32_t o = 0;
@@ -171,14 +171,28 @@ __device__ __forceinline__ void block2_fixed(const float *__restrict__ alpha, co
 #pragma unroll
         for (int p = 0; p < P; ++p)
             path[p] = alpha + (base[p] + aoff_reg(r, a) + (in.TA[p] >> (kTB - a)) * plen_reg(r, a) +
-                               (in.TB[p] >> (kTB - L)) * (uint32_t)(L + 1));
+                               (in.TB[p] >> (kTB - L)) * (uint32_t)SG_PATH_WIDTH(L + 1));
         FV<P> sr = FV<P>::all(0.0f);
+        /* slots 2j, 2j+1 in one 8-byte load (paths of L >= 1 start even) */
 #pragma unroll
-        for (int b = 0; b <= L; ++b) {
+        for (int b = 0; b + 1 <= L; b += 2) {
+            float2 w[P];
+#pragma unroll
+            for (int p = 0; p < P; ++p) w[p] = __ldg(reinterpret_cast<const float2 *>(path[p] + b));
+            FV<P> v0, v1;
+#pragma unroll
+            for (int p = 0; p < P; ++p) {
+                v0.set(p, w[p].x);
+                v1.set(p, w[p].y);
+            }
+            sr = vfma(in.hB[b], v0, sr);
+            sr = vfma(in.hB[b + 1], v1, sr);
+        }
+        if ((L & 1) == 0) {
             FV<P> v;
 #pragma unroll
-            for (int p = 0; p < P; ++p) v.set(p, __ldg(path[p] + b));
-            sr = vfma(in.hB[b], v, sr);
+            for (int p = 0; p < P; ++p) v.set(p, __ldg(path[p] + L));
+            sr = vfma(in.hB[L], v, sr);
         }
         s = (a == 0) ? vmul(in.hA(0), sr) : vfma(in.hA(a), sr, s);
     }
@@ -224,14 +238,15 @@ __device__ __forceinline__ void block2_generic(const float *__restrict__ alpha, 
             }
         }
         const int rl = min(r - a, limB) + 1;
-        const uint32_t plen = (1u << (rl - 1)) * (uint32_t)rl;
+        const uint32_t plen = (1u << (rl - 1)) * (uint32_t)SG_PATH_WIDTH(rl);
         FV<P> yB, sr = FV<P>::all(0.0f);
         uint32_t rb[P];
 #pragma unroll
         for (int p = 0; p < P; ++p) {
             yB.set(p, xB[p]);
             /* path of the finest cell t_L = floor(x_B 2^L), exact */
-            rb[p] = base[p] + aoff + tA[p] * plen + (uint32_t)(xB[p] * (float)(1u << (rl - 1))) * (uint32_t)rl;
+            rb[p] = base[p] + aoff + tA[p] * plen +
+                    (uint32_t)(xB[p] * (float)(1u << (rl - 1))) * (uint32_t)SG_PATH_WIDTH(rl);
         }
         for (int b = 0; b < rl; ++b) {
             if (b) {

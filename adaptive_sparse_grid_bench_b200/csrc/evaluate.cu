@@ -61,7 +61,7 @@ __global__ void k_repack(const float *__restrict__ src, float *__restrict__ dst,
         const int ab = r.a + r.b, cab = r.c + ab;
         const int rep = r.L - r.b; /* the value fills slot b of 2^rep paths */
         const int n = 1 << (r.s + rep);
-        const uint32_t w = (uint32_t)r.L + 1u;
+        const uint32_t w = (uint32_t)SG_PATH_WIDTH(r.L + 1);
         for (int f = threadIdx.x & 31; f < n; f += 32) {
             const uint32_t e = (uint32_t)f >> rep, j = (uint32_t)f & ((1u << rep) - 1u);
             const uint32_t I = e >> cab;

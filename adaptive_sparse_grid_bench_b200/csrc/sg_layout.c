@@ -230,7 +230,7 @@ void sg_layout_eval_sub(const sg_layout *L, int r, sg_eval_sub *sh)
         sh->rowlen[a] = rl + 1;
         sh->aoff[a] = off;
         /* 2^a poles of 2^rl paths of rl+1 slots */
-        off += ((uint32_t)1 << a) * (((uint32_t)1 << rl) * (uint32_t)(rl + 1));
+        off += ((uint32_t)1 << a) * (((uint32_t)1 << rl) * (uint32_t)SG_PATH_WIDTH(rl + 1));
     }
     sh->aoff[sh->amax + 1] = off;
 }
@@ -334,7 +334,7 @@ int sg_layout_eval_tables(const sg_layout *L, sg_repack **repack, uint32_t *blk3
             rp[r].dst = (uint32_t)base + sh.coff[c] + sub.aoff[a] + (uint32_t)b;
             rp[r].blk = sh.coff[sh.cmax + 1];
             rp[r].sub = sub.aoff[sub.amax + 1];
-            rp[r].plen = ((uint32_t)1 << (sub.rowlen[a] - 1)) * (uint32_t)sub.rowlen[a];
+            rp[r].plen = ((uint32_t)1 << (sub.rowlen[a] - 1)) * (uint32_t)SG_PATH_WIDTH(sub.rowlen[a]);
             rp[r].L = (uint8_t)(sub.rowlen[a] - 1);
             rp[r].pad[0] = rp[r].pad[1] = rp[r].pad[2] = 0;
             rp[r].c = (uint8_t)c;

@@ -71,12 +71,19 @@ int sg_layout_chains(const sg_layout *L, int k, sg_chain **chains, int64_t *ncha
  *   (one per cell t_a of dim A);
  *   a pole holds dim B's levels b = 0..L (L = rowlen-1) as 2^L paths, one
  *   per finest cell t_L: path t_L is the L+1 surpluses a query point in that
- *   cell needs, level b's cell t_L >> (L-b) in slot b.  A surplus of level
- *   b therefore appears in 2^(L-b) paths (Nblk >= N values in all).
+ *   cell needs, level b's cell t_L >> (L-b) in slot b, in W = L+1 rounded up
+ *   to even slots (SG_PATH_WIDTH).  A surplus of level b therefore appears
+ *   in 2^(L-b) paths (Nblk >= N values in all).
  * A query point finds the surplus of (c, a, b) at
- *   base + coff(c) + t_c * sub(R-c) + aoff(R-c, a) + t_a * plen + t_L * (L+1) + b,
- * so the L+1 loads of a row share one address and differ by a constant.
+ *   base + coff(c) + t_c * sub(R-c) + aoff(R-c, a) + t_a * plen + t_L * W + b,
+ * so the loads of a row share one address and differ by a constant; every
+ * row with L >= 1 starts at an even offset (all sizes before it in a block
+ * are even), so slots 2j, 2j+1 move with one 8-byte load.
  */
+/* Slots of a path of `levels` levels: rounded up to an even count (two
+ * levels per 8-byte load), a single level alone. */
+#define SG_PATH_WIDTH(levels) ((levels) <= 1 ? (levels) : (((levels) + 1) & ~1))
+
 typedef struct sg_eval_sub {
     int amax;                         /* last row: min(r, lim_A)           */
     int rowlen[SG_MAX_LEVELS];        /* levels of dim B in row a           */

@@ -84,7 +84,7 @@ SG_API int sg_batch_create(int num_grids, const int *dims, const int *levels, co
         b->boff[g] = boff;
         voff += b->L[g].N;
         doff += b->L[g].Npad;
-        boff += b->L[g].Nblk;
+        boff += (b->L[g].Nblk + 1) & ~(int64_t)1; /* grids start even: 8-byte path loads */
     }
     b->voff[num_grids] = voff;
     b->doff[num_grids] = doff;
