@@ -4,7 +4,7 @@ evaluation on sm_100a behind the C ABI of include/sgrid.h.
 The compute lives in libsgb200.so (CUDA kernels + C host code); this package
 only binds it (`Grid`) and generates seeded inputs (`inputs`).
 """
-from ._lib import (SG_HIER_FP32, SG_HIER_FP64, SG_OPT_EVAL_PPT,  # noqa: F401
+from ._lib import (SG_HIER_FP32, SG_HIER_FP64, SG_OPT_EVAL_BLOCKING, SG_OPT_EVAL_PPT,  # noqa: F401
                    SG_OPT_EVAL_SORT, SG_OPT_HIER_KERNEL, SG_OPT_HIER_PRECISION, SG_OPT_PROFILE, SgError,
                    header_functions, lib)
 from .batch import Batch  # noqa: F401

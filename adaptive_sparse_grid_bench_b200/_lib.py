@@ -33,6 +33,8 @@ SG_OPT_PROFILE = 6
 SG_OPT_USE_GRAPH = 7
 SG_OPT_SWEEP_GROUP = 8
 SG_OPT_TEST_WAIT = 9
+SG_OPT_EVAL_BLOCKING = 10
+SG_EVAL_BLOCKINGS = 2
 SG_SRV_OPT_ZERO_COPY = 1
 SG_SRV_OPT_HEAVY_PAIRS = 2
 SG_SRV_OPT_LIGHT_SLOTS = 3
@@ -46,7 +48,8 @@ SG_FN_BUMP = 3
 SG_FN_QUAD = 4
 
 SG_MAX_DIMS = 20
-SG_TUNE_TIMINGS = 6
+SG_TUNE_TIMINGS = 8
+SG_BATCH_TUNE_TIMINGS = 4 * (SG_MAX_DIMS + 1)
 SG_MAX_LEVELS = 16
 SG_NOALLOC_MAX_POINTS = 1 << 18
 SG_NOALLOC_SCRATCH_BYTES = 24 << 20

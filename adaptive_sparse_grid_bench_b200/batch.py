@@ -100,13 +100,14 @@ class Batch:
         check(L.lib().sg_batch_sync(self._h, _stream_handle(stream)))
 
     def autotune(self, point_offsets, coords, out, stream=None) -> np.ndarray:
-        """sg_batch_autotune: per dimension, the faster of 1 and 2 points per
-        thread on these buffers; returns ms[ppt-1][d] (-1 = no grid of d)."""
+        """sg_batch_autotune: per dimension, the fastest pair of points per
+        thread (1, 2) and subspace blocking (1 wide, 2 medium) on
+        these buffers; returns ms[blocking-1][ppt-1][d] (-1 = no grid of d)."""
         po = np.ascontiguousarray(point_offsets, np.int64)
         if po.shape != (self.num_grids + 1,):
             raise ValueError("point_offsets needs num_grids + 1 entries")
         self._po = po
-        ms = np.zeros((2, L.SG_MAX_DIMS + 1), np.float64)
+        ms = np.zeros((L.SG_EVAL_BLOCKINGS, 2, L.SG_MAX_DIMS + 1), np.float64)
         check(L.lib().sg_batch_autotune(self._h, po.ctypes.data, int(coords.data_ptr()), int(out.data_ptr()),
                                         _stream_handle(stream), ms.ctypes.data))
         return ms

@@ -2,6 +2,6 @@
  * so the instantiations compile in parallel. */
 #include "eval_impl.cuh"
 
-template int eval_launch<1>(const EvalArgs &, int, void *);
+template int eval_launch<1>(const EvalArgs &, int, int, void *);
 template int eval_setup<1>();
-template int eval_batch_launch<1>(const EvalArgs *, const int2 *, int, int, void *);
+template int eval_batch_launch<1>(const EvalArgs *, const int2 *, int, int, int, void *);

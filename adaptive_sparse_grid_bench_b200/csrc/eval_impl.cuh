@@ -28,18 +28,23 @@
  *     __fmul2_rn): one instruction does both points' FMA, product or
  *     compensated add, with each point's rounding exactly as in scalar code,
  *     so results are bit-identical to one point per thread;
- *   - blocks of budget R <= kRF run fully unrolled; larger blocks loop over
- *     their planes and run each plane's 2-D sub-block fully unrolled behind a
- *     jump table.  A block or sub-block whose budget is within the limits of
+ *   - blocks of budget R <= kRFof<BL> run fully unrolled; larger blocks
+ *     loop over their planes and run each plane's 2-D sub-block fully
+ *     unrolled behind a jump table.  A block or sub-block whose budget is within the limits of
  *     its dims has the regular shape whatever the limits, so limit-vector
  *     (adaptive) grids take the unrolled code too; a generic loop covers
  *     budgets above the limits, budgets >= kNB and d = 1;
  *   - most blocks sit under walk nodes of small remaining budget (at d=10,
  *     n=10, 8,008 of 11,440 blocks hold at most 4 subspaces), where loop and
  *     dispatch cost more than the gathers: the last prefix dim with budget
- *     <= kLG (levels and blocks) and the last two with budget <= 3 run as
- *     fully unrolled code with compile-time block sizes, in walk order, so
- *     results are bit-identical to the loop (d <= kMaxUnrollD);
+ *     <= kLGof<P, BL> (levels and blocks) and the last two with budget
+ *     <= kLG2 run as fully unrolled code with compile-time block sizes, in
+ *     walk order, so results are bit-identical to the loop (d <= kMaxUnrollD);
+ *   - BL is the subspace blocking preset, a template parameter (wide = 0,
+ *     medium = 1; the autotuner picks one per grid or per dimension of a
+ *     batch): more unrolled code saves loop and dispatch work but raises
+ *     register pressure, and the best trade depends on the grid and on the
+ *     kernel (the batched kernel holds more state);
  *   - per prefix dim the walk keeps three values per point: the fractional
  *     part y = frac(x 2^l) (next level: doubling, exact in FP32), the cell
  *     index of the prefix (next level: 2*ix + bit) and the parent's product;
@@ -61,7 +66,11 @@ namespace sgeval {
 
 constexpr int kThreads = 256;
 constexpr int kNB = 10; /* 2-D sub-blocks of budget r < kNB run fully unrolled */
-constexpr int kRF = 5;  /* 3-D blocks of budget R <= kRF run fully unrolled    */
+constexpr int kRF = SG_EVAL_MAX_RF; /* 3-D blocks of budget R <= kRF can run unrolled */
+static_assert(kRF == 6, "block_sum's jump table covers budgets 0..6");
+/* largest budget of an unrolled 3-D block under blocking preset BL */
+template <int BL>
+constexpr int kRFof = BL == 0 ? kRF : 5;
 constexpr int kTB = 15; /* T = floor(x 2^15) holds the cells of levels 0..15   */
 
 /* P floats of one thread's points: float2 (packed FP32x2 instructions) for
@@ -286,20 +295,26 @@ __device__ __forceinline__ void block2_any(const EvalArgs &A, int r, const Inner
 }
 
 /* Sum over the block of budget R at `base` for every point. */
-template <int D, int P>
+template <int D, int P, int BL>
 __device__ __forceinline__ void block_sum(const EvalArgs &A, int R, const Inner<P> &in, const float (&xC)[P],
                                           const float (&xA)[P], const float (&xB)[P], const uint32_t (&base)[P],
                                           FV<P> &s)
 {
     if constexpr (D >= 3) {
-        if (R <= kRF && R <= A.lim3) {
+        if (R <= kRFof<BL> && R <= A.lim3) {
             switch (R) {
             case 0: block3_planes<0, 0, P>(A.alpha, base, in, s); return;
             case 1: block3_planes<1, 0, P>(A.alpha, base, in, s); return;
             case 2: block3_planes<2, 0, P>(A.alpha, base, in, s); return;
             case 3: block3_planes<3, 0, P>(A.alpha, base, in, s); return;
             case 4: block3_planes<4, 0, P>(A.alpha, base, in, s); return;
-            default: block3_planes<kRF, 0, P>(A.alpha, base, in, s); return;
+            case 5:
+                if constexpr (kRFof<BL> > 5) {
+                    block3_planes<5, 0, P>(A.alpha, base, in, s);
+                    return;
+                }
+                [[fallthrough]];
+            default: block3_planes<kRFof<BL>, 0, P>(A.alpha, base, in, s); return;
             }
         }
     }
@@ -347,7 +362,14 @@ struct Range {
     bool partial;
 };
 
-constexpr int kLG = 3;
+/* largest budget of an unrolled leaf subtree: of the last prefix dim
+ * (kLGof, per points per thread under the wide preset: two points need
+ * twice the registers), of the last two (kLG2) */
+template <int P, int BL>
+constexpr int kLGof = BL == 0 ? (P == 1 ? SG_EVAL_MAX_LEAF_P1 : SG_EVAL_MAX_LEAF_P2) : 3;
+constexpr int kLG2 = SG_EVAL_MAX_LEAF2;
+static_assert(SG_EVAL_MAX_LEAF_P1 <= 5 && SG_EVAL_MAX_LEAF_P2 <= 5 && kLG2 <= 3,
+              "the walk's jump tables cover leaf budgets 0..5 and 0..3");
 /* unrolled subtrees are instantiated for d <= kMaxUnrollD only (their code
  * grows with d; grids of more dims keep the loop) */
 constexpr int kMaxUnrollD = 12;
@@ -415,9 +437,12 @@ __device__ __forceinline__ void leaf_group2(const EvalArgs &A, const float *sx, 
 }
 
 /* Walk over prefix dim K (K <= D-4); children of depth D-4 are blocks.
- * SPLIT: the caller may ask for a block range (batched launches). */
-template <int D, int K, int P, bool SPLIT>
+ * M = mode: bit 0 (SPLIT) = the caller may ask for a block range (batched
+ * launches), bits 1.. (BL) = the blocking preset. */
+template <int D, int K, int P, int M>
 struct Walk {
+    static constexpr bool SPLIT = (M & 1) != 0;
+    static constexpr int BL = M >> 1;
     static __device__ __forceinline__ void run(const EvalArgs &A, const float *sx, int tid, int budget,
                                                uint32_t &cur, Range &rg, const Inner<P> &in, const float (&xC)[P],
                                                const float (&xA)[P], const float (&xB)[P], const FV<P> &pin,
@@ -463,7 +488,7 @@ struct Walk {
                     }
                 }
                 const FV<P> pn = vmul(pp, hats(y));
-                Walk<D, K + 1, P, SPLIT>::run(A, sx, tid, budget - l, cur, rg, in, xC, xA, xB, pn, ix, sum, comp);
+                Walk<D, K + 1, P, M>::run(A, sx, tid, budget - l, cur, rg, in, xC, xA, xB, pn, ix, sum, comp);
             }
             return;
         }
@@ -474,7 +499,7 @@ struct Walk {
 #pragma unroll
         for (int p = 0; p < P; ++p) ix[p] = ixin[p];
         if constexpr (D <= kMaxUnrollD && K + 1 == D - 4) {
-            if (!(SPLIT && rg.partial) && budget <= 3 && budget <= A.lim[K] && budget <= A.lim[K + 1] &&
+            if (!(SPLIT && rg.partial) && budget <= kLG2 && budget <= A.lim[K] && budget <= A.lim[K + 1] &&
                 budget <= A.lim3) {
                 switch (budget) {
                 case 0: leaf_group2<D, K, P, 0, 0>(A, sx, tid, cur, in, pin, y, ix, sum, comp); break;
@@ -487,12 +512,18 @@ struct Walk {
             }
         }
         if constexpr (D <= kMaxUnrollD && K == D - 4) {
-            if (!(SPLIT && rg.partial) && budget <= kLG && budget <= A.lim[K] && budget <= A.lim3) {
+            if (!(SPLIT && rg.partial) && budget <= kLGof<P, BL> && budget <= A.lim[K] && budget <= A.lim3) {
                 switch (budget) {
                 case 0: leaf_group<D, P, 0, 0>(A, cur, in, pin, y, ix, acc); break;
                 case 1: leaf_group<D, P, 1, 0>(A, cur, in, pin, y, ix, acc); break;
                 case 2: leaf_group<D, P, 2, 0>(A, cur, in, pin, y, ix, acc); break;
                 case 3: leaf_group<D, P, 3, 0>(A, cur, in, pin, y, ix, acc); break;
+                case 4:
+                    if constexpr (kLGof<P, BL> >= 4) leaf_group<D, P, 4, 0>(A, cur, in, pin, y, ix, acc);
+                    break;
+                case 5:
+                    if constexpr (kLGof<P, BL> >= 5) leaf_group<D, P, 5, 0>(A, cur, in, pin, y, ix, acc);
+                    break;
                 default: break;
                 }
                 kahan_add(sum, comp, acc);
@@ -522,10 +553,10 @@ struct Walk {
                 for (int p = 0; p < P; ++p) base[p] = cur + ix[p] * blk;
                 cur += blk << (A.nm1 - R);
                 if (SPLIT) ++rg.leaf;
-                block_sum<D, P>(A, R, in, xC, xA, xB, base, s);
+                block_sum<D, P, BL>(A, R, in, xC, xA, xB, base, s);
                 acc = vfma(pn, s, acc);
             } else {
-                Walk<D, K + 1, P, SPLIT>::run(A, sx, tid, budget - l, cur, rg, in, xC, xA, xB, pn, ix, sum, comp);
+                Walk<D, K + 1, P, M>::run(A, sx, tid, budget - l, cur, rg, in, xC, xA, xB, pn, ix, sum, comp);
             }
         }
         if constexpr (K == D - 4) kahan_add(sum, comp, acc);
@@ -535,10 +566,11 @@ struct Walk {
 /* Evaluates this thread's points first, first + 32, ..., first + 32(P-1)
  * (those below `end`) against grid A; sx is this CTA's shared coordinate
  * buffer, shat its shared hats of dims A and C. */
-template <int D, int P, bool SPLIT>
+template <int D, int P, int M>
 __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, FV<P> *shat, int tid, int64_t first,
                                             int64_t end, int part)
 {
+    constexpr bool SPLIT = (M & 1) != 0;
     float xC[P], xA[P], xB[P];
     bool valid[P], nan_in[P];
 #pragma unroll
@@ -627,13 +659,13 @@ __device__ __forceinline__ void eval_points(const EvalArgs &A, float *sx, FV<P> 
         rg.partial = SPLIT && A.nparts > 1;
         rg.lo = rg.partial ? A.split[part] : 0u;
         rg.hi = rg.partial ? A.split[part + 1] : 0xFFFFFFFFu;
-        Walk<D, 0, P, SPLIT>::run(A, sx, tid, A.nm1, cur, rg, in, xC, xA, xB, pin, ix, sum, comp);
+        Walk<D, 0, P, M>::run(A, sx, tid, A.nm1, cur, rg, in, xC, xA, xB, pin, ix, sum, comp);
     } else {
         uint32_t base[P];
         FV<P> s;
 #pragma unroll
         for (int p = 0; p < P; ++p) base[p] = 0;
-        block_sum<D, P>(A, A.nm1, in, xC, xA, xB, base, s);
+        block_sum<D, P, (M >> 1)>(A, A.nm1, in, xC, xA, xB, base, s);
         kahan_add(sum, comp, s);
     }
 
@@ -657,7 +689,18 @@ template <int D, int P>
 constexpr int kSmemBytes = kHatSlots * kThreads * (int)sizeof(FV<P>) + (D >= 4 ? D - 3 : 1) * P * kThreads * 4 +
                            kUpper<D> * 3 * P * kThreads * 4;
 
-template <int D, int P>
+/* blocking presets instantiated for dimension D: both where the leaf
+ * groups and 3-D blocks exist (3 <= D <= kMaxUnrollD); elsewhere one,
+ * kBaseBL<D>: medium above kMaxUnrollD (no leaf groups; the wide preset's
+ * larger 3-D blocks only add spills to those kernels' large walk state),
+ * wide below 3 (no 3-D blocks: the presets are the same code) */
+template <int D>
+constexpr int kBlockings = (D >= 3 && D <= kMaxUnrollD) ? SG_EVAL_BLOCKINGS : 1;
+template <int D>
+constexpr int kBaseBL = D > kMaxUnrollD ? 1 : 0;
+static_assert(SG_EVAL_BLOCKINGS == 2, "presets: wide (0) and medium (1)");
+
+template <int D, int P, int BL>
 __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const EvalArgs A)
 {
     extern __shared__ __align__(16) unsigned char smem_ev[];
@@ -665,13 +708,13 @@ __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3)) k_evaluate(const E
     float *sx = reinterpret_cast<float *>(smem_ev + kHatSlots * kThreads * sizeof(FV<P>));
     const int tid = threadIdx.x;
     const int64_t warp = (blockIdx.x * (int64_t)kThreads + tid) >> 5;
-    eval_points<D, P, false>(A, sx, shat, tid, warp * (32 * P) + (tid & 31), A.num_evals, 0);
+    eval_points<D, P, 2 * BL>(A, sx, shat, tid, warp * (32 * P) + (tid & 31), A.num_evals, 0);
 }
 
 /* Many grids of the same dimension in one launch: CTA b evaluates the
  * kThreads*P points of grid items[b].x & (2^29-1) starting at point
  * items[b].y; bits 29..31 of items[b].x select the part of a split sum. */
-template <int D, int P>
+template <int D, int P, int BL>
 __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3))
     k_evaluate_batch(const EvalArgs *__restrict__ grids, const int2 *__restrict__ items)
 {
@@ -690,18 +733,40 @@ __global__ void __launch_bounds__(kThreads, (P == 2 ? 2 : 3))
     __syncthreads();
     const int64_t start = item.y;
     const int64_t end = min(start + (int64_t)kThreads * P, sA.num_evals);
-    eval_points<D, P, true>(sA, sx, shat, tid, start + (tid >> 5) * (32 * P) + (tid & 31), end, part);
+    eval_points<D, P, 2 * BL + 1>(sA, sx, shat, tid, start + (tid >> 5) * (32 * P) + (tid & 31), end, part);
 }
 
-template <int D, int P>
+template <int D, int P, int BL>
 int launch_eval(const EvalArgs &A, void *stream)
 {
     const int64_t per_block = (int64_t)kThreads * P;
     const int64_t blocks = (A.num_evals + per_block - 1) / per_block;
     if (blocks > 0x7fffffff) return cudaErrorInvalidValue;
-    k_evaluate<D, P><<<(unsigned)blocks, kThreads, kSmemBytes<D, P>, (cudaStream_t)stream>>>(A);
+    k_evaluate<D, P, BL><<<(unsigned)blocks, kThreads, kSmemBytes<D, P>, (cudaStream_t)stream>>>(A);
     sgk_count(1);
     return cudaGetLastError();
+}
+
+template <int D, int P, int BL>
+int launch_eval_batch(const EvalArgs *grids, const int2 *items, int nitems, void *stream)
+{
+    k_evaluate_batch<D, P, BL><<<nitems, kThreads, kSmemBytes<D, P>, (cudaStream_t)stream>>>(grids, items);
+    sgk_count(1);
+    return cudaGetLastError();
+}
+
+template <int D, int BL>
+int set_smem(void)
+{
+    int e = cudaFuncSetAttribute(k_evaluate<D, 1, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes<D, 1>);
+    if (!e) e = cudaFuncSetAttribute(k_evaluate<D, 2, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes<D, 2>);
+    if (!e)
+        e = cudaFuncSetAttribute(k_evaluate_batch<D, 1, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kSmemBytes<D, 1>);
+    if (!e)
+        e = cudaFuncSetAttribute(k_evaluate_batch<D, 2, BL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kSmemBytes<D, 2>);
+    return e;
 }
 
 } // namespace sgeval
@@ -712,36 +777,33 @@ int launch_eval(const EvalArgs &A, void *stream)
 template <int D>
 int eval_setup()
 {
-    int e = cudaFuncSetAttribute(sgeval::k_evaluate<D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 sgeval::kSmemBytes<D, 1>);
-    if (!e) e = cudaFuncSetAttribute(sgeval::k_evaluate<D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     sgeval::kSmemBytes<D, 2>);
-    if (!e) e = cudaFuncSetAttribute(sgeval::k_evaluate_batch<D, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     sgeval::kSmemBytes<D, 1>);
-    if (!e) e = cudaFuncSetAttribute(sgeval::k_evaluate_batch<D, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     sgeval::kSmemBytes<D, 2>);
+    int e = sgeval::set_smem<D, sgeval::kBaseBL<D>>();
+    if constexpr (sgeval::kBlockings<D> > 1)
+        if (!e) e = sgeval::set_smem<D, 1>();
     return e;
 }
 
+/* blocking: preset index; dimensions with one form take kBaseBL<D> */
 template <int D>
-int eval_launch(const EvalArgs &A, int ppt, void *stream)
+int eval_launch(const EvalArgs &A, int ppt, int blocking, void *stream)
 {
-    if (ppt == 1) return sgeval::launch_eval<D, 1>(A, stream);
-    return sgeval::launch_eval<D, 2>(A, stream);
+    constexpr int B0 = sgeval::kBaseBL<D>;
+    if constexpr (sgeval::kBlockings<D> > 1)
+        if (blocking == 1) return ppt == 1 ? sgeval::launch_eval<D, 1, 1>(A, stream) : sgeval::launch_eval<D, 2, 1>(A, stream);
+    return ppt == 1 ? sgeval::launch_eval<D, 1, B0>(A, stream) : sgeval::launch_eval<D, 2, B0>(A, stream);
 }
 
 template <int D>
-int eval_batch_launch(const EvalArgs *grids, const int2 *items, int nitems, int ppt, void *stream)
+int eval_batch_launch(const EvalArgs *grids, const int2 *items, int nitems, int ppt, int blocking, void *stream)
 {
     if (nitems <= 0) return cudaSuccess;
-    if (ppt == 1)
-        sgeval::k_evaluate_batch<D, 1>
-            <<<nitems, sgeval::kThreads, sgeval::kSmemBytes<D, 1>, (cudaStream_t)stream>>>(grids, items);
-    else
-        sgeval::k_evaluate_batch<D, 2>
-            <<<nitems, sgeval::kThreads, sgeval::kSmemBytes<D, 2>, (cudaStream_t)stream>>>(grids, items);
-    sgk_count(1);
-    return cudaGetLastError();
+    if constexpr (sgeval::kBlockings<D> > 1)
+        if (blocking == 1)
+            return ppt == 1 ? sgeval::launch_eval_batch<D, 1, 1>(grids, items, nitems, stream)
+                            : sgeval::launch_eval_batch<D, 2, 1>(grids, items, nitems, stream);
+    constexpr int B0 = sgeval::kBaseBL<D>;
+    return ppt == 1 ? sgeval::launch_eval_batch<D, 1, B0>(grids, items, nitems, stream)
+                    : sgeval::launch_eval_batch<D, 2, B0>(grids, items, nitems, stream);
 }
 
 #endif

@@ -289,10 +289,10 @@ int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm
     if (num_evals <= 0) return cudaSuccess;
     EvalArgs A;
     sgk_fill_eval_args(p, coords, perm, out, num_evals, &A);
-    const int ppt = p->ppt;
+    const int ppt = p->ppt, bl = p->blocking >= 0 && p->blocking < SG_EVAL_BLOCKINGS ? p->blocking : 0;
     switch (p->d) {
 #define SG_D(DD) \
-    case DD: return eval_launch<DD>(A, ppt, stream);
+    case DD: return eval_launch<DD>(A, ppt, bl, stream);
         SG_D(1) SG_D(2) SG_D(3) SG_D(4) SG_D(5) SG_D(6) SG_D(7) SG_D(8) SG_D(9) SG_D(10)
         SG_D(11) SG_D(12) SG_D(13) SG_D(14) SG_D(15) SG_D(16) SG_D(17) SG_D(18) SG_D(19)
         SG_D(20)
@@ -301,12 +301,14 @@ int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm
     }
 }
 
-int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, int nitems, int ppt, void *stream)
+int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, int nitems, int ppt, int blocking,
+                       void *stream)
 {
     const int2 *it = reinterpret_cast<const int2 *>(items);
+    const int bl = blocking >= 0 && blocking < SG_EVAL_BLOCKINGS ? blocking : 0;
     switch (d) {
 #define SG_D(DD) \
-    case DD: return eval_batch_launch<DD>(grids, it, nitems, ppt, stream);
+    case DD: return eval_batch_launch<DD>(grids, it, nitems, ppt, bl, stream);
         SG_D(1) SG_D(2) SG_D(3) SG_D(4) SG_D(5) SG_D(6) SG_D(7) SG_D(8) SG_D(9) SG_D(10)
         SG_D(11) SG_D(12) SG_D(13) SG_D(14) SG_D(15) SG_D(16) SG_D(17) SG_D(18) SG_D(19)
         SG_D(20)

@@ -71,6 +71,9 @@ struct sg_batch {
     int32_t *d_perm;                 /* sorted position -> caller's local index    */
     int ppt_d[SG_MAX_DIMS + 1];      /* points per thread per dimension (0: ppt) */
     int eval_ppt_d[SG_MAX_DIMS + 1]; /* the setting the current plan was built for */
+    int blocking;                    /* SG_OPT_EVAL_BLOCKING (0: auto = wide)       */
+    int blk_d[SG_MAX_DIMS + 1];      /* tuned blocking per dimension (0: blocking) */
+    int eval_blk_d[SG_MAX_DIMS + 1]; /* the setting the current plan was built for */
     int *order;                      /* grids by dimension, most subspaces first */
     /* the per-dimension launches of an evaluation fork onto their own
      * streams (joined back before the caller's stream continues) */

@@ -9,7 +9,7 @@
 #include "sg_kernels.h"
 #include "sg_layout.h"
 
-#define NOPT 10
+#define NOPT 11
 
 /* Device allocator hooks.  A handle made by sg_create uses cudaMalloc and
  * cudaFree; the serving loop hands its grids a sub-allocator over one

@@ -67,7 +67,16 @@ typedef struct sg_eval_plan {
     uint32_t blk3[SG_MAX_LEVELS]; /* block size for each level budget R      */
     uint32_t blk2[SG_MAX_LEVELS]; /* sub-block size for each level budget r  */
     int ppt;                     /* points per thread (1 or 2)               */
+    int blocking;                /* subspace blocking preset, 0 .. SG_EVAL_BLOCKINGS-1
+                                    (wide, medium)                            */
 } sg_eval_plan;
+
+/* Subspace blocking presets of the evaluation kernels (SG_OPT_EVAL_BLOCKING
+ * 1..2 select preset 0..1): how much of the walk runs as fully unrolled
+ * blocks of compile-time shape (separate kernel instantiations for
+ * 3 <= d <= 12; other d have one form).  Every preset gives bit-identical
+ * results. */
+#define SG_EVAL_BLOCKINGS 2
 
 /* A point's sum over the subspaces can be split into up to this many
  * parts (ranges of the walk's blocks), evaluated by separate CTAs and added
@@ -115,8 +124,9 @@ int sgk_evaluate(const sg_eval_plan *p, const float *coords, const int32_t *perm
 /* Many grids of dimension d in one launch: items (device, 2 ints per CTA) =
  * (index into grids | part << 29, first point); each CTA covers
  * SG_EVAL_CTA_POINTS(ppt) points of its grid (index < 2^29; part selects
- * the block range of a split sum, 0 for whole sums). */
-int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, int nitems, int ppt,
+ * the block range of a split sum, 0 for whole sums); blocking is the
+ * preset index of the launch (0 .. SG_EVAL_BLOCKINGS-1). */
+int sgk_evaluate_batch(int d, const sg_eval_args *grids, const int32_t *items, int nitems, int ppt, int blocking,
                        void *stream);
 
 /* out[i] = compensated sum over k < nparts of part_out[k * num_evals + i]

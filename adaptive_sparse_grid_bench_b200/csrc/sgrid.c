@@ -585,6 +585,13 @@ SG_API int sg_autotune(sg_grid *g, const float *coords, float *out, int64_t num_
         g->opt[SG_OPT_EVAL_PPT] = ppts[bi / 2];
         g->opt[SG_OPT_EVAL_SORT] = bi % 2;
     }
+    /* subspace blocking at that setting (scratch and layout are built) */
+    for (i = 0, best = 1e30, bi = -1; i < SG_EVAL_BLOCKINGS && r == SG_OK; i++) {
+        g->opt[SG_OPT_EVAL_BLOCKING] = i + 1;
+        r = time_best(tune_eval_once, g, &ta, ta.st, 2, &t[6 + i]);
+        if (r == SG_OK && t[6 + i] < best) best = t[6 + i], bi = i;
+    }
+    if (r == SG_OK) g->opt[SG_OPT_EVAL_BLOCKING] = bi + 1;
     /* hierarchization: shared-memory chains (where they fit) vs gather; the
      * values are saved first and restored at the end */
     for (k = 0; k < g->L.d; k++)
@@ -656,24 +663,33 @@ static int eval_ppt(const sg_grid *g)
     return 2;
 }
 
+/* The evaluation plan of the grid's block layout at `ppt` points per
+ * thread and the grid's blocking setting (0 = auto: wide). */
+static void grid_plan(const sg_grid *g, int ppt, sg_eval_plan *p)
+{
+    int k;
+    p->alpha = g->d_blk;
+    p->d = g->L.d;
+    p->n = g->L.n;
+    for (k = 0; k < SG_MAX_DIMS; k++) p->lim[k] = k < g->L.d ? g->L.lim[k] : 0;
+    for (k = 0; k < SG_MAX_LEVELS; k++) {
+        p->blk3[k] = g->blk3[k];
+        p->blk2[k] = g->blk2[k];
+    }
+    p->ppt = ppt;
+    p->blocking = g->opt[SG_OPT_EVAL_BLOCKING] > 0 ? (int)g->opt[SG_OPT_EVAL_BLOCKING] - 1 : 0;
+}
+
 static int evaluate_on(sg_grid *g, const float *coords, float *out, int64_t m, cudaStream_t st)
 {
     sg_eval_plan p;
-    int e, k;
+    int e;
     if (g->eval_dirty) {
         if ((e = sgk_repack(g->d_alpha, g->d_blk, g->d_repack, g->L.S, st)) != cudaSuccess)
             return cuda_fail((cudaError_t)e, "repacking surpluses");
         g->eval_dirty = 0;
     }
-    p.alpha = g->d_blk;
-    p.d = g->L.d;
-    p.n = g->L.n;
-    for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < g->L.d ? g->L.lim[k] : 0;
-    for (k = 0; k < SG_MAX_LEVELS; k++) {
-        p.blk3[k] = g->blk3[k];
-        p.blk2[k] = g->blk2[k];
-    }
-    p.ppt = eval_ppt(g);
+    grid_plan(g, eval_ppt(g), &p);
     if (g->opt[SG_OPT_EVAL_SORT] && m > 1) {
         const int64_t sort_b = (sgk_sort_scratch_bytes(m, p.d) + 255) & ~(int64_t)255;
         const int64_t coords_b = (m * p.d * 4 + 255) & ~(int64_t)255;
@@ -747,15 +763,7 @@ SG_API int sg_evaluate_device_noalloc(sg_grid *g, const float *coords, float *ou
                 g->eval_dirty = 0;
         }
         if (r == SG_OK) {
-            p.alpha = g->d_blk;
-            p.d = g->L.d;
-            p.n = g->L.n;
-            for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < g->L.d ? g->L.lim[k] : 0;
-            for (k = 0; k < SG_MAX_LEVELS; k++) {
-                p.blk3[k] = g->blk3[k];
-                p.blk2[k] = g->blk2[k];
-            }
-            p.ppt = eval_ppt(g);
+            grid_plan(g, eval_ppt(g), &p);
             /* the histogram is cleared inside the sort, so nothing left in
              * the shared array by an earlier call is read */
             if ((e = sgk_sort_points(coords, m, p.d, base, sorted, perm, st)) != cudaSuccess)
@@ -881,6 +889,9 @@ SG_API int sg_set_option(sg_grid *g, int option, int64_t value)
     case SG_OPT_TEST_WAIT:
         if (value < 0 || value > 2048) return fail(SG_ERR_ARG, "SG_OPT_TEST_WAIT is 0 .. 2048");
         break;
+    case SG_OPT_EVAL_BLOCKING:
+        if (value < 0 || value > SG_EVAL_BLOCKINGS) return fail(SG_ERR_ARG, "SG_OPT_EVAL_BLOCKING is 0 .. %d", SG_EVAL_BLOCKINGS);
+        break;
     default:
         return fail(SG_ERR_ARG, "unknown option %d", option);
     }
@@ -954,15 +965,7 @@ void sg_grid_eval_args(const sg_grid *g, const float *coords, float *out, int64_
 {
     sg_eval_plan p;
     int k;
-    p.alpha = g->d_blk;
-    p.d = g->L.d;
-    p.n = g->L.n;
-    for (k = 0; k < SG_MAX_DIMS; k++) p.lim[k] = k < g->L.d ? g->L.lim[k] : 0;
-    for (k = 0; k < SG_MAX_LEVELS; k++) {
-        p.blk3[k] = g->blk3[k];
-        p.blk2[k] = g->blk2[k];
-    }
-    p.ppt = 2;
+    grid_plan(g, 2, &p);
     sgk_fill_eval_args(&p, coords, NULL, out, m, a);
     if (g->nparts > 1) {
         a->nparts = g->nparts;

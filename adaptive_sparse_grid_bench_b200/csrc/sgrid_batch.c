@@ -766,6 +766,12 @@ SG_API int sg_batch_hierarchize(sg_batch *b)
  * the caller's point offsets and buffers (kept, so an identical call replays
  * the captured graph). */
 static int ppt_of(const sg_batch *b, int d) { return b->ppt_d[d] ? b->ppt_d[d] : b->ppt; }
+/* blocking preset index (0 .. SG_EVAL_BLOCKINGS-1) of dimension d */
+static int blk_of(const sg_batch *b, int d)
+{
+    const int v = b->blk_d[d] ? b->blk_d[d] : b->blocking;
+    return v > 0 ? v - 1 : 0;
+}
 
 static int cmp_dim_then_subspaces(const void *x, const void *y, void *ctx)
 {
@@ -854,7 +860,7 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
     int g, k, r, q;
     int64_t coff = 0, ni = 0, cap_items = 0;
     int same = b->h_eval_args && b->eval_coords == coords && b->eval_out == out && b->eval_sort == b->sort;
-    for (k = 0; same && k <= SG_MAX_DIMS; k++) same = b->eval_ppt_d[k] == ppt_of(b, k);
+    for (k = 0; same && k <= SG_MAX_DIMS; k++) same = b->eval_ppt_d[k] == ppt_of(b, k) && b->eval_blk_d[k] == blk_of(b, k);
     for (g = 0; same && g <= b->ng; g++) same = b->eval_pt_off[g] == pt_off[g];
     if (same) return SG_OK;
     if (b->eval_graph) {
@@ -904,6 +910,7 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
             }
         }
         p.ppt = ppt_of(b, L->d);
+        p.blocking = blk_of(b, L->d);
         sgk_fill_eval_args(&p, coords + coff, NULL, out + pt_off[g], pt_off[g + 1] - pt_off[g], &b->h_eval_args[g]);
         coff += (pt_off[g + 1] - pt_off[g]) * L->d;
     }
@@ -937,7 +944,10 @@ static int plan_eval(sg_batch *b, const int64_t *pt_off, const float *coords, fl
     for (g = 0; g <= b->ng; g++) b->eval_pt_off[g] = pt_off[g];
     b->eval_coords = coords;
     b->eval_out = out;
-    for (k = 0; k <= SG_MAX_DIMS; k++) b->eval_ppt_d[k] = ppt_of(b, k);
+    for (k = 0; k <= SG_MAX_DIMS; k++) {
+        b->eval_ppt_d[k] = ppt_of(b, k);
+        b->eval_blk_d[k] = blk_of(b, k);
+    }
     b->eval_sort = b->sort;
     return SG_OK;
 }
@@ -970,7 +980,7 @@ static int eval_launches(sg_batch *b, cudaStream_t st)
         if (!b->items_count[k]) continue;
         BCU(cudaStreamWaitEvent(b->dst[k], b->ev_fork, 0), "cudaStreamWaitEvent");
         e = sgk_evaluate_batch(k, b->d_eval_args, b->d_items + 2 * (int64_t)b->items_first[k], b->items_count[k],
-                               ppt_of(b, k), b->dst[k]);
+                               ppt_of(b, k), blk_of(b, k), b->dst[k]);
         if (e != cudaSuccess) return bcuda((cudaError_t)e, "batch evaluate");
         BCU(cudaEventRecord(b->ev_d[k], b->dst[k]), "cudaEventRecord");
         BCU(cudaStreamWaitEvent(st, b->ev_d[k], 0), "cudaStreamWaitEvent");
@@ -1000,23 +1010,28 @@ SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const fl
 {
     cudaStream_t st = (cudaStream_t)stream;
     cudaEvent_t e0 = NULL, e1 = NULL;
-    double t[2][SG_MAX_DIMS + 1];
-    int prev, r, pi, k, q, rep;
+    double t[2 * SG_EVAL_BLOCKINGS][SG_MAX_DIMS + 1];
+    int prev, r, pi, k, q, rep, cfg;
     float el;
     if (!b || !point_offsets || point_offsets[0] != 0) return bfail(SG_ERR_ARG, "sg_batch_autotune: bad argument");
     if (!b->has_values || b->dev < 0) return bfail(SG_ERR_STATE, "sg_batch_autotune: no values have been set");
     if (point_offsets[b->ng] > 0 && (!coords || !out)) return bfail(SG_ERR_ARG, "sg_batch_autotune: NULL buffer");
     if ((r = enter(b, &prev)) != SG_OK) return r;
-    for (pi = 0; pi < 2; pi++)
-        for (k = 0; k <= SG_MAX_DIMS; k++) t[pi][k] = -1.0;
+    for (cfg = 0; cfg < 2 * SG_EVAL_BLOCKINGS; cfg++)
+        for (k = 0; k <= SG_MAX_DIMS; k++) t[cfg][k] = -1.0;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
         r = bfail(SG_ERR_CUDA, "sg_batch_autotune: cudaEventCreate");
         goto done;
     }
     if ((r = make_fork_streams(b)) != SG_OK) goto done;
-    /* every dimension's launch alone on st, at 1 and at 2 points per thread */
-    for (pi = 0; pi < 2 && r == SG_OK; pi++) {
-        for (k = 0; k <= SG_MAX_DIMS; k++) b->ppt_d[k] = pi + 1;
+    /* every dimension's launch alone on st, at 1 and at 2 points per thread
+     * (pi) under each blocking preset (cfg / 2) */
+    for (cfg = 0; cfg < 2 * SG_EVAL_BLOCKINGS && r == SG_OK; cfg++) {
+        pi = cfg % 2;
+        for (k = 0; k <= SG_MAX_DIMS; k++) {
+            b->ppt_d[k] = pi + 1;
+            b->blk_d[k] = cfg / 2 + 1;
+        }
         if ((r = plan_eval(b, point_offsets, coords, out)) != SG_OK) break;
         if (b->sort && sgk_batch_sort_points(coords, b->d_sgrids, b->d_sitems, b->nsitems, b->sort_npts, b->sort_nbins,
                                              b->d_sscratch, b->d_sorted, b->d_perm, st) != cudaSuccess) {
@@ -1032,18 +1047,23 @@ SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const fl
             for (rep = 0; rep < 3; rep++) { /* first run warms */
                 if (cudaEventRecord(e0, st) != cudaSuccess ||
                     sgk_evaluate_batch(k, b->d_eval_args, b->d_items + 2 * (int64_t)b->items_first[k],
-                                       b->items_count[k], pi + 1, st) != cudaSuccess ||
+                                       b->items_count[k], pi + 1, cfg / 2, st) != cudaSuccess ||
                     cudaEventRecord(e1, st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
                     cudaEventElapsedTime(&el, e0, e1) != cudaSuccess) {
                     r = bfail(SG_ERR_CUDA, "sg_batch_autotune: timing d=%d", k);
                     break;
                 }
-                if (rep > 0 && (t[pi][k] < 0.0 || el < t[pi][k])) t[pi][k] = el;
+                if (rep > 0 && (t[cfg][k] < 0.0 || el < t[cfg][k])) t[cfg][k] = el;
             }
         }
     }
-    for (k = 0; k <= SG_MAX_DIMS; k++)
-        b->ppt_d[k] = (r == SG_OK && t[0][k] >= 0.0) ? (t[0][k] <= t[1][k] ? 1 : 2) : 0;
+    for (k = 0; k <= SG_MAX_DIMS; k++) {
+        int best = -1;
+        for (cfg = 0; r == SG_OK && cfg < 2 * SG_EVAL_BLOCKINGS; cfg++)
+            if (t[cfg][k] >= 0.0 && (best < 0 || t[cfg][k] < t[best][k])) best = cfg;
+        b->ppt_d[k] = best >= 0 ? best % 2 + 1 : 0;
+        b->blk_d[k] = best >= 0 ? best / 2 + 1 : 0;
+    }
     b->eval_dirty = 1;
     /* sweeps: per chain size class, the staged chain kernel or one warp per
      * chain (both bit-identical); the values are saved and restored */
@@ -1097,8 +1117,8 @@ SG_API int sg_batch_autotune(sg_batch *b, const int64_t *point_offsets, const fl
         }
     }
     if (ms)
-        for (pi = 0; pi < 2; pi++)
-            for (k = 0; k <= SG_MAX_DIMS; k++) ms[pi * (SG_MAX_DIMS + 1) + k] = t[pi][k];
+        for (cfg = 0; cfg < 2 * SG_EVAL_BLOCKINGS; cfg++)
+            for (k = 0; k <= SG_MAX_DIMS; k++) ms[cfg * (SG_MAX_DIMS + 1) + k] = t[cfg][k];
 done:
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -1122,6 +1142,12 @@ SG_API int sg_batch_set_option(sg_batch *b, int option, int64_t value)
         if (value < 0 || value > 2) return bfail(SG_ERR_ARG, "SG_OPT_EVAL_PPT is 0, 1 or 2");
         b->ppt = value == 0 ? 2 : (int)value;
         memset(b->ppt_d, 0, sizeof(b->ppt_d)); /* an explicit setting replaces tuned ones */
+        return SG_OK;
+    case SG_OPT_EVAL_BLOCKING:
+        if (value < 0 || value > SG_EVAL_BLOCKINGS)
+            return bfail(SG_ERR_ARG, "SG_OPT_EVAL_BLOCKING is 0 .. %d", SG_EVAL_BLOCKINGS);
+        b->blocking = (int)value;
+        memset(b->blk_d, 0, sizeof(b->blk_d));
         return SG_OK;
     case SG_OPT_USE_GRAPH:
         if (value != 0 && value != 1) return bfail(SG_ERR_ARG, "SG_OPT_USE_GRAPH is 0 or 1");

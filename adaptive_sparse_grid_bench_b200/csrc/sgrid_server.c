@@ -482,7 +482,7 @@ static int launch_batch(sg_server *s, srv_slot *sl)
     for (d = 1; d <= SG_MAX_DIMS; d++) {
         if (!count[d]) continue;
         if (cudaStreamWaitEvent(sl->dst[d], sl->ev_in, 0) != cudaSuccess) return SG_ERR_CUDA;
-        e = sgk_evaluate_batch(d, sl->d_args, sl->d_items + 2 * (int64_t)first[d], count[d], ppt[d], sl->dst[d]);
+        e = sgk_evaluate_batch(d, sl->d_args, sl->d_items + 2 * (int64_t)first[d], count[d], ppt[d], 0, sl->dst[d]);
         if (e != cudaSuccess || cudaEventRecord(sl->ev_d[d], sl->dst[d]) != cudaSuccess ||
             cudaStreamWaitEvent(sl->st, sl->ev_d[d], 0) != cudaSuccess)
             return SG_ERR_CUDA;

@@ -235,7 +235,8 @@ class Grid:
         check(L.lib().sg_autotune(self._h, self._dptr(coords), self._dptr(out), int(num_evals),
                                   _stream_handle(stream), _ptr(ms)))
         return {"eval_ppt1_unsorted": ms[0], "eval_ppt1_sorted": ms[1], "eval_ppt2_unsorted": ms[2],
-                "eval_ppt2_sorted": ms[3], "hier_chains": ms[4], "hier_gather": ms[5]}
+                "eval_ppt2_sorted": ms[3], "hier_chains": ms[4], "hier_gather": ms[5],
+                "eval_blocking_wide": ms[6], "eval_blocking_medium": ms[7]}
 
     def idx2gp_device(self, index, levels, indices, count: int, stream=None) -> None:
         check(L.lib().sg_idx2gp_device(self._h, self._dptr(index), self._dptr(levels), self._dptr(indices),

@@ -58,8 +58,8 @@ EVAL_SRC = os.path.join(ROOT, "adaptive_sparse_grid_bench_b200", "csrc", "eval_i
 #     2^24-point launch (one-pass metrics, so the full launch was captured);
 #   inst_per_pair: smsp__inst_executed.sum x 32 / (points x subspaces) of a
 #     262,144-point launch of the same grid.
-EVAL_CAPTURE = {"source_sha16": "44f82de6e967df93", "captured": "2026-12-04", "dram_bytes": 2.032e9 + 0.556e9,
-                "inst_per_pair": 10.41}
+EVAL_CAPTURE = {"source_sha16": "0789b8dc88ff7494", "captured": "2026-12-04", "dram_bytes": 2.919e9 + 0.601e9,
+                "inst_per_pair": 8.10}
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -426,8 +426,8 @@ def capture_figures():
 def run_b200(args, rank: int, world: int, local_rank: int, wl=None, extras: bool = False, err: bool = False):
     import torch
     import torch.distributed as dist
-    from adaptive_sparse_grid_bench_b200._lib import (SG_OPT_EVAL_PPT, SG_OPT_EVAL_SORT, SG_OPT_HIER_KERNEL,
-                                                      SG_OPT_PROFILE, kernel_launches)
+    from adaptive_sparse_grid_bench_b200._lib import (SG_OPT_EVAL_BLOCKING, SG_OPT_EVAL_PPT, SG_OPT_EVAL_SORT,
+                                                      SG_OPT_HIER_KERNEL, SG_OPT_PROFILE, kernel_launches)
 
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
@@ -445,6 +445,7 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None, extras: bool
     # this workload's own buffers (no setting changes a result)
     tuned = g.autotune(X_d, out_d, m, stream)
     tuned["chosen"] = {"ppt": g.get_option(SG_OPT_EVAL_PPT), "sort": g.get_option(SG_OPT_EVAL_SORT),
+                       "blocking": g.get_option(SG_OPT_EVAL_BLOCKING),
                        "hier_kernel": g.get_option(SG_OPT_HIER_KERNEL)}
     t_hier, t_eval, t_sort = [], [], []
 
@@ -607,8 +608,12 @@ def run_batched(args, rank: int, world: int, local_rank: int):
     stream.wait_stream(torch.cuda.current_stream())
     b.set_values_device(vals, stream)
     b.hierarchize_async(stream)
-    tuned = b.autotune(po, X, out, stream)  # points per thread per dimension
-    tuned_ppt = {d: (1 if tuned[0, d] <= tuned[1, d] else 2) for d in range(tuned.shape[1]) if tuned[0, d] >= 0}
+    tuned = b.autotune(po, X, out, stream)  # points per thread and blocking per dimension
+    tuned_ppt = {}
+    for d in range(tuned.shape[2]):
+        if tuned[0, 0, d] >= 0:
+            bl, pp = np.unravel_index(int(np.argmin(tuned[:, :, d])), tuned.shape[:2])
+            tuned_ppt[d] = {"ppt": int(pp) + 1, "blocking": int(bl) + 1}
     npts = [inputs.regular_grid_size(int(d), int(n))[0] for d, n in zip(dims, levels)]
 
     def step():
@@ -690,7 +695,7 @@ def run_batched(args, rank: int, world: int, local_rank: int):
         "evaluate": {"ms": statistics.mean(te), "evals_per_s": total_pts / (statistics.mean(te) / 1e3)},
         "plain_per_grid": {"evals_per_s": plain_value, "grids_sampled": len(sample),
                            "note": "one set_values/hierarchize/evaluate launch sequence per grid, summed"},
-        "speedup_vs_plain": value / plain_value, "autotuned_ppt_by_d": tuned_ppt,
+        "speedup_vs_plain": value / plain_value, "autotuned_by_d": tuned_ppt,
         "gpu_launches": int(launches), "clocks": clk.summary(),
     }
     if err is not None:
@@ -1014,7 +1019,7 @@ def run_extras(args, rank: int, world: int, local_rank: int) -> dict:
     a.grids = 1024
     out["batched"] = compact(run_batched(a, rank, world, local_rank),
                              ["value", "unit", "ms_per_step", "config", "hierarchize", "evaluate", "plain_per_grid",
-                              "speedup_vs_plain", "err_vs_fp64", "gpu_launches"])
+                              "speedup_vs_plain", "autotuned_by_d", "err_vs_fp64", "gpu_launches"])
     a = copy.copy(args)
     a.rates, a.requests = "16000,20000,24000,28000", 3000
     srv = run_served(a, rank, world, local_rank)
@@ -1029,7 +1034,7 @@ def run_extras(args, rank: int, world: int, local_rank: int) -> dict:
     a.steps, a.warmup, a.no_e2e, a.no_cpu_baseline, a.points = min(args.steps, 10), 3, True, True, None
     out["adaptive"] = compact(run_b200(a, rank, world, local_rank, adaptive_workload(a), err=True),
                               ["value", "unit", "ms_per_step", "config", "hierarchize", "evaluate", "err_vs_fp64",
-                               "gpu_launches"])
+                               "autotune_ms", "gpu_launches"])
     return out
 
 

@@ -75,6 +75,14 @@ extern "C" {
                                 /* k * 2^20 clock cycles (about k/2 ms); the next     */
                                 /* sg_sync returns SG_ERR_TIMEOUT and the values are  */
                                 /* invalid.  0 (default): off.                       */
+#define SG_OPT_EVAL_BLOCKING 10 /* evaluate: how much of the subspace walk runs as   */
+                                /* fully unrolled blocks of compile-time shape:      */
+                                /* 1 = wide (3-D blocks of level budget <= 6, leaf  */
+                                /* subtrees of budget <= 5 at one point per thread  */
+                                /* or <= 4 at two), 2 = medium (5, 3); 0 = auto    */
+                                /* (wide, or the tuned choice).  Grids of d < 3 or  */
+                                /* d > 12 have one form.  Results are bit-identical */
+                                /* under every setting.                             */
 
 /* Phases reported by sg_timings (milliseconds of the most recent call). */
 #define SG_PHASE_HIERARCHIZE 0  /* all sweeps of the last hierarchization    */
@@ -153,15 +161,17 @@ int sg_sync(sg_grid *grid, void *stream);
 /* Autotuner (no reference counterpart; the reference tunes its CUDA block
  * size by hand, run.sh).  Times, on the caller's device buffers and stream,
  * the evaluation under every setting of points per thread {1, 2} x spatial
- * ordering {off, on}, and the hierarchization with the shared-memory chain
- * sweeps (where they fit) and the gather sweeps; keeps the fastest in the
- * handle's options (SG_OPT_EVAL_PPT, SG_OPT_EVAL_SORT, SG_OPT_HIER_KERNEL).
- * No setting changes any result.  The grid's values are the same on return
- * (saved and restored); out[] holds the evaluation.  ms (optional,
- * SG_TUNE_TIMINGS entries): evaluation ms for (ppt, sort) = (1,0), (1,1),
- * (2,0), (2,1), then hierarchization ms for chains and gather (-1: not
+ * ordering {off, on}, then, at the faster of those, under every subspace
+ * blocking (SG_OPT_EVAL_BLOCKING 1..2), and the hierarchization with the
+ * shared-memory chain sweeps (where they fit) and the gather sweeps; keeps
+ * the fastest in the handle's options (SG_OPT_EVAL_PPT, SG_OPT_EVAL_SORT,
+ * SG_OPT_EVAL_BLOCKING, SG_OPT_HIER_KERNEL).  No setting changes any result.
+ * The grid's values are the same on return (saved and restored); out[] holds
+ * the evaluation.  ms (optional, SG_TUNE_TIMINGS entries): evaluation ms for
+ * (ppt, sort) = (1,0), (1,1), (2,0), (2,1), then hierarchization ms for
+ * chains and gather, then evaluation ms for blocking 1, 2 (-1: not
  * applicable). */
-#define SG_TUNE_TIMINGS 6
+#define SG_TUNE_TIMINGS 8
 int sg_autotune(sg_grid *grid, const float *coord_mat, float *out, int64_t num_evals, void *stream, double *ms);
 
 /* Device bijection for batches (no reference counterpart beyond looping
@@ -244,16 +254,20 @@ int sg_batch_evaluate_device(sg_batch *batch, const int64_t *point_offsets, cons
 int sg_batch_sync(sg_batch *batch, void *stream);
 /* SG_OPT_HIER_PRECISION, SG_OPT_EVAL_PPT, SG_OPT_USE_GRAPH, SG_OPT_HIER_KERNEL (sweeps),
  * SG_OPT_EVAL_SORT (1, default: each grid's points spatially ordered on the GPU),
- * SG_OPT_SWEEP_GROUP (before the first device call; SG_ERR_STATE after it) */
+ * SG_OPT_EVAL_BLOCKING, SG_OPT_SWEEP_GROUP (before the first device call;
+ * SG_ERR_STATE after it) */
 int sg_batch_set_option(sg_batch *batch, int option, int64_t value);
 /* Autotuner for batches (no reference counterpart): times each
  * dimension's evaluation launch over the caller's points at 1 and at 2
- * points per thread and keeps the faster per dimension, and times the
+ * points per thread under each subspace blocking (SG_OPT_EVAL_BLOCKING
+ * 1..2) and keeps the fastest pair per dimension, and times the
  * hierarchization with each chain size class on the staged chain kernel and
  * on one warp per chain and keeps the faster per class (the values are
- * saved and restored).  Results do not change.  An SG_OPT_EVAL_PPT or
- * SG_OPT_HIER_KERNEL setting replaces the tuned choice.  ms (optional,
- * 2*(SG_MAX_DIMS+1) entries): [ppt-1][d] launch ms, -1 where no grid has d. */
+ * saved and restored).  Results do not change.  An SG_OPT_EVAL_PPT,
+ * SG_OPT_EVAL_BLOCKING or SG_OPT_HIER_KERNEL setting replaces the tuned
+ * choice.  ms (optional, SG_BATCH_TUNE_TIMINGS entries):
+ * [(blocking-1)*2 + ppt-1][d] launch ms, -1 where no grid has d. */
+#define SG_BATCH_TUNE_TIMINGS (4 * (SG_MAX_DIMS + 1))
 int sg_batch_autotune(sg_batch *batch, const int64_t *point_offsets, const float *coord_mat, float *out,
                       void *stream, double *ms);
 int sg_batch_device_bytes(const sg_batch *batch, int64_t *bytes);

@@ -35,11 +35,15 @@ def test_header_constants_match_bindings():
     text = open(_lib.HEADER).read()
     for name in ["SG_MAX_DIMS", "SG_MAX_LEVELS", "SG_OK", "SG_HIER_FP64", "SG_OPT_HIER_PRECISION",
                  "SG_OPT_EVAL_SORT", "SG_OPT_EVAL_PPT", "SG_OPT_HIER_KERNEL", "SG_OPT_PROFILE",
-                 "SG_OPT_USE_GRAPH", "SG_OPT_SWEEP_GROUP", "SG_FN_GAUSS", "SG_FN_QUAD", "SG_NUM_PHASES"]:
+                 "SG_OPT_USE_GRAPH", "SG_OPT_SWEEP_GROUP", "SG_OPT_TEST_WAIT", "SG_OPT_EVAL_BLOCKING",
+                 "SG_TUNE_TIMINGS", "SG_FN_GAUSS", "SG_FN_QUAD", "SG_NUM_PHASES"]:
         import re
         m = re.search(rf"#define {name} \(?(-?\d+)\)?", text)
         assert m, name
         assert int(m.group(1)) == getattr(_lib, name), name
+    m = re.search(r"#define SG_BATCH_TUNE_TIMINGS \((\d+) \* \(SG_MAX_DIMS \+ 1\)\)", text)
+    assert m and int(m.group(1)) * (_lib.SG_MAX_DIMS + 1) == _lib.SG_BATCH_TUNE_TIMINGS
+    assert int(m.group(1)) == 2 * _lib.SG_EVAL_BLOCKINGS
 
 
 @pytest.mark.parametrize("name", golden_cases())
@@ -116,9 +120,14 @@ def test_options_validate():
     grid.precision = "fp64"
     assert grid.precision == "fp64"
     for opt, bad in [(sg.SG_OPT_HIER_PRECISION, 2), (sg.SG_OPT_EVAL_SORT, 3), (sg.SG_OPT_EVAL_PPT, 5),
-                     (sg.SG_OPT_HIER_KERNEL, -1), (99, 0)]:
+                     (sg.SG_OPT_HIER_KERNEL, -1), (sg.SG_OPT_EVAL_BLOCKING, -1), (sg.SG_OPT_EVAL_BLOCKING, 4),
+                     (99, 0)]:
         with pytest.raises(sg.SgError):
             grid.set_option(opt, bad)
+    assert grid.get_option(sg.SG_OPT_EVAL_BLOCKING) == 0  # auto
+    for ok in range(_lib.SG_EVAL_BLOCKINGS + 1):
+        grid.set_option(sg.SG_OPT_EVAL_BLOCKING, ok)
+        assert grid.get_option(sg.SG_OPT_EVAL_BLOCKING) == ok
 
 
 def test_batch_sweep_group_option_validates():
@@ -129,6 +138,11 @@ def test_batch_sweep_group_option_validates():
     for bad in (-1, 1 << 32):
         with pytest.raises(sg.SgError):
             b.set_option(_lib.SG_OPT_SWEEP_GROUP, bad)
+    for ok in range(_lib.SG_EVAL_BLOCKINGS + 1):
+        b.set_option(_lib.SG_OPT_EVAL_BLOCKING, ok)
+    for bad in (-1, _lib.SG_EVAL_BLOCKINGS + 1):
+        with pytest.raises(sg.SgError):
+            b.set_option(_lib.SG_OPT_EVAL_BLOCKING, bad)
     b.close()
 
 

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import adaptive_sparse_grid_bench_b200 as sg
-from adaptive_sparse_grid_bench_b200 import inputs
+from adaptive_sparse_grid_bench_b200 import _lib, inputs
 from conftest import golden_cases, load_golden
 from oracle.oracle import Oracle
 
@@ -113,6 +113,28 @@ def test_evaluate_vs_fp64_oracle(cuda, d, n, lim, ppt):
     for sort in (1, 0):
         g.set_option(sg.SG_OPT_EVAL_SORT, sort)
         assert_eval_close(g.evaluate(X), ref64, f"d={d} n={n} sort={sort} ppt={ppt}")
+
+
+@pytest.mark.parametrize("d,n,lim", [(10, 8, None), (4, 12, None), (6, 9, [8, 2, 5, 8, 8, 1]), (3, 12, [11, 4, 9]),
+                                     (12, 6, None), (5, 10, [9, 9, 9, 3, 9])])
+def test_blocking_presets_bit_identical(cuda, d, n, lim):
+    # every subspace blocking (wide, medium) at one and two points
+    # per thread gives the same bits, and they are within tolerance of FP64
+    o = Oracle(d, n, lim)
+    g = _grid(d, n, lim)
+    g.set_values(inputs.grid_values(g, inputs.f_gauss))
+    g.hierarchize()
+    X = inputs.uniform_points(17, 3000, d)
+    outs = {}
+    for blocking in range(1, _lib.SG_EVAL_BLOCKINGS + 1):
+        for ppt in (1, 2):
+            g.set_option(sg.SG_OPT_EVAL_BLOCKING, blocking)
+            g.set_option(sg.SG_OPT_EVAL_PPT, ppt)
+            outs[blocking, ppt] = g.evaluate(X)
+    first = outs[1, 1]
+    for key, out in outs.items():
+        assert np.array_equal(out.view(np.uint32), first.view(np.uint32)), f"blocking, ppt = {key}"
+    assert_eval_close(first, o.evaluate_f64(g.get_values().astype(np.float64), X), f"d={d} n={n}")
 
 
 def test_evaluate_edge_coordinates(cuda):
@@ -243,6 +265,7 @@ def test_autotune_keeps_values_and_results(cuda, d, n, lim, precision):
     assert np.array_equal(out.cpu().numpy().view(np.uint32), want.view(np.uint32))
     assert g.get_option(sg.SG_OPT_EVAL_PPT) in (1, 2) and g.get_option(sg.SG_OPT_EVAL_SORT) in (0, 1)
     assert g.get_option(sg.SG_OPT_HIER_KERNEL) in (1, 2)
+    assert g.get_option(sg.SG_OPT_EVAL_BLOCKING) in (1, 2, 3)
     assert np.array_equal(g.evaluate(X).view(np.uint32), want.view(np.uint32))
     # the tuned sweep kernel still gives hierarchize0's bits
     g.set_values(inputs.uniform01(7, g.num_points) * 2 - 1)
