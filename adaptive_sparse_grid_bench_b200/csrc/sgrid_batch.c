@@ -622,11 +622,39 @@ static int sweep_class(sg_batch *b, const sg_sweep_tables *t, int c, int fp64, c
     return e == cudaSuccess ? SG_OK : bcuda((cudaError_t)e, "batch sweep");
 }
 
+/* The shared-memory hierarchization of the small grids, one launch per size
+ * class, on stream hs. */
+static int smem_launches(sg_batch *b, int fp64, cudaStream_t hs)
+{
+    int c;
+    for (c = 0; c < SG_BATCH_CLASSES; c++) {
+        cudaError_t e;
+        if (!b->cls_count[c]) continue;
+        e = (cudaError_t)sgk_hier_smem_grids(b->d_alpha, b->d_smem_grids + b->cls_first[c], b->cls_count[c],
+                                             b->d_smem_chains, b->d_smem_seg, b->cls_max_npad[c], fp64, hs);
+        if (e != cudaSuccess) return bcuda(e, "batch shared-memory hierarchization");
+    }
+    return SG_OK;
+}
+
 static int hier_launches(sg_batch *b, cudaStream_t st)
 {
-    int k, c, q, r;
+    int k, c, q, r, any_smem = 0;
     cudaError_t e;
     const int fp64 = b->precision == SG_HIER_FP64;
+    /* FP32: the sweeps touch only their own grids' values, so the small
+     * grids' shared-memory launches run on a stream of their own beside them
+     * (joined back at the end); FP64 runs them after the sweeps, whose
+     * widen/narrow round trip rewrites the whole buffer */
+    const cudaStream_t hs = b->dst[SG_MAX_DIMS];
+    for (c = 0; c < SG_BATCH_CLASSES; c++) any_smem |= b->cls_count[c] > 0;
+    const int beside = !fp64 && any_smem && b->has_sweep_grids;
+    if (beside) {
+        BCU(cudaEventRecord(b->ev_fork, st), "cudaEventRecord");
+        BCU(cudaStreamWaitEvent(hs, b->ev_fork, 0), "cudaStreamWaitEvent");
+        if ((r = smem_launches(b, fp64, hs)) != SG_OK) return r;
+        BCU(cudaEventRecord(b->ev_d[SG_MAX_DIMS], hs), "cudaEventRecord");
+    }
     if (b->has_sweep_grids) {
         if (fp64 && (e = (cudaError_t)sgk_widen(b->d_alpha, b->d_work, b->doff[b->ng], st)) != cudaSuccess)
             return bcuda(e, "widen");
@@ -672,15 +700,13 @@ static int hier_launches(sg_batch *b, cudaStream_t st)
         if (fp64 && (e = (cudaError_t)sgk_narrow(b->d_work, b->d_alpha, b->doff[b->ng], st)) != cudaSuccess)
             return bcuda(e, "narrow");
     }
+    if (beside) {
+        BCU(cudaStreamWaitEvent(st, b->ev_d[SG_MAX_DIMS], 0), "cudaStreamWaitEvent");
+        return SG_OK;
+    }
     /* after the sweeps: their FP64 round trip rewrites the whole buffer with
      * the (unchanged) nodal values of the shared-memory grids */
-    for (c = 0; c < SG_BATCH_CLASSES; c++) {
-        if (!b->cls_count[c]) continue;
-        e = (cudaError_t)sgk_hier_smem_grids(b->d_alpha, b->d_smem_grids + b->cls_first[c], b->cls_count[c],
-                                             b->d_smem_chains, b->d_smem_seg, b->cls_max_npad[c], fp64, st);
-        if (e != cudaSuccess) return bcuda(e, "batch shared-memory hierarchization");
-    }
-    return SG_OK;
+    return smem_launches(b, fp64, st);
 }
 
 /* Replays *exec, capturing body into it first.  The library's launch
