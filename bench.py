@@ -584,7 +584,7 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None, extras: bool
     elif world == 1 and err:
         line["err_vs_fp64"] = error_vs_fp64(vals_d.cpu().numpy(), out_d.cpu().numpy(), X, nsample=256, wl=wl)
     if world == 1 and extras:
-        line["reference_gpu"] = reference_gpu(g, X, out_d.cpu().numpy())
+        line["reference_gpu"] = reference_gpu(g, X, out_d.cpu().numpy(), nodal=vals_d.cpu().numpy())
     del X_d, out_d, vals_d
     g.close()
     return line
@@ -994,12 +994,16 @@ def compact(line: dict | None, keys) -> dict | None:
     return None if line is None else {k: line[k] for k in keys if k in line}
 
 
-def reference_gpu(g, X: np.ndarray, ours: np.ndarray, m: int = 1 << 18) -> dict:
+def reference_gpu(g, X: np.ndarray, ours: np.ndarray, m: int = 1 << 18, nodal: np.ndarray | None = None) -> dict:
     """The reference's own CUDA evaluation kernel (evaluate5, cu:1522-1598,
     compiled in place by oracle/ref_cuda_harness.cu) on the same hierarchized
     grid and the first m query points, points per warp swept over the values
     its run script uses (run.sh:14-18).  kernel: its kernel alone; copies: its
-    own timed region (coordinates in, kernel, results out, cu:1829-1897)."""
+    own timed region (coordinates in, kernel, results out, cu:1829-1897).
+    With the nodal values, also its hierarchization (hierarchize7,
+    cu:1053-1160, with the warp barriers it lacks added) of the whole grid:
+    the median of 3 runs after one warm-up, and whether its surpluses are
+    bit-identical to this library's."""
     from oracle.oracle import ReferenceCUDA
     if not ReferenceCUDA.available():
         return {"unavailable": "oracle/_ref/libasgb_refcuda.so not built"}
@@ -1018,7 +1022,18 @@ def reference_gpu(g, X: np.ndarray, ours: np.ndarray, m: int = 1 << 18) -> dict:
     tt = statistics.median(r[1] for r in runs)
     scale = float(np.max(np.abs(ours[:m])))
     pairs = m * g.num_subspaces / (tk / 1e3)
-    return {"kernel": "reference evaluate5 (cu:1522-1598)", "points": m, "points_per_warp": P,
+    hier = None
+    if nodal is not None and 6 <= g.n <= 10:
+        hout = ReferenceCUDA.hierarchize7(g.d, g.n, nodal, reps=1)[0]
+        hruns = [ReferenceCUDA.hierarchize7(g.d, g.n, nodal, reps=1)[1:] for _ in range(3)]
+        hk = statistics.median(r[0] for r in hruns)
+        ht = statistics.median(r[1] for r in hruns)
+        hier = {"kernel": "reference hierarchize7 (cu:1053-1160), one launch per dimension",
+                "kernel_ms": hk, "copies_ms": ht, "timing": "median of 3 runs",
+                "gbs_kernel": 8.0 * g.d * g.num_points / (hk / 1e3) / 1e9, "bytes": "8*d*N",
+                "ref_gflops_kernel": hi_gflops(g.d, g.num_points, hk),
+                "bitexact_vs_b200": bool(np.array_equal(hout.view(np.uint32), surplus.view(np.uint32)))}
+    return {"kernel": "reference evaluate5 (cu:1522-1598)", "hierarchize": hier, "points": m, "points_per_warp": P,
             "kernel_ms": tk, "copies_ms": tt, "timing": "median of 5 runs at the best points per warp",
             "evals_per_s_kernel": m / (tk / 1e3),
             "evals_per_s_copies": m / (tt / 1e3), "pairs_per_s_kernel": pairs,

@@ -213,11 +213,13 @@ class Reference:
 
 
 class ReferenceCUDA:
-    """The reference's CUDA evaluate5 kernel (adaptive_sparse_grid_bench_cuda.cu:1522),
-    compiled in place (``_ref/libasgb_refcuda.so``); timed next to this
-    project's kernels.  The harness refuses sizes outside the kernel's safe
-    launch conditions (P a multiple of 32, points a multiple of 8 P, n <= 10,
-    d <= 20, coordinates in [0,1)) before touching the GPU."""
+    """The reference's CUDA kernels evaluate5 (adaptive_sparse_grid_bench_cuda.cu:1522)
+    and hierarchize7 (cu:1053, with the warp barriers it lacks added by
+    ``patch_ref_cuda.py``), compiled into ``_ref/libasgb_refcuda.so``; timed
+    next to this project's kernels.  The harness refuses sizes outside each
+    kernel's safe launch conditions before touching the GPU: for evaluate5
+    P a multiple of 32, points a multiple of 8 P, n <= 10, d <= 20,
+    coordinates in [0,1); for hierarchize7 6 <= n <= 10, d <= 20."""
 
     _lib = None
 
@@ -232,6 +234,9 @@ class ReferenceCUDA:
             lib.refcuda_evaluate5.argtypes = [C.c_int, C.c_int, _fp, C.c_int, _fp, C.c_int, C.c_int, C.c_int, _fp,
                                               C.POINTER(C.c_float), C.POINTER(C.c_float)]
             lib.refcuda_evaluate5.restype = C.c_int
+            lib.refcuda_hierarchize7.argtypes = [C.c_int, C.c_int, _fp, C.c_int, C.c_int, _fp,
+                                                 C.POINTER(C.c_float), C.POINTER(C.c_float)]
+            lib.refcuda_hierarchize7.restype = C.c_int
             cls._lib = lib
         return cls._lib
 
@@ -246,4 +251,17 @@ class ReferenceCUDA:
                                         C.byref(tt))
         if r != 0:
             raise RuntimeError(f"refcuda_evaluate5 returned {r}")
+        return out, tk.value, tt.value
+
+    @classmethod
+    def hierarchize7(cls, d: int, n: int, values, reps: int = 1):
+        """Hierarchizes the nodal values (compact order) with the reference's
+        hierarchize7, one launch per dimension as its main() does.  Returns
+        (surpluses, fastest kernel ms, fastest ms with the copy in)."""
+        a = np.ascontiguousarray(values, np.float32)
+        out = np.zeros(a.size, np.float32)
+        tk, tt = C.c_float(), C.c_float()
+        r = cls.lib().refcuda_hierarchize7(d, n, a, a.size, reps, out, C.byref(tk), C.byref(tt))
+        if r != 0:
+            raise RuntimeError(f"refcuda_hierarchize7 returned {r}")
         return out, tk.value, tt.value

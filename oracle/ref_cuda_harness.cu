@@ -1,9 +1,10 @@
 /*
- * Harness that compiles the REFERENCE CUDA benchmark in place and exports
- * its evaluate5 kernel (adaptive_sparse_grid_bench_cuda.cu:1522-1598) for
- * timing next to this project's kernels.  TEST INFRASTRUCTURE ONLY: built by
- * oracle/Makefile into oracle/_ref/ (never committed); no reference source is
- * copied into this repository; REF_CU names the file where it lies.
+ * Harness that compiles the REFERENCE CUDA benchmark and exports its
+ * evaluate5 (adaptive_sparse_grid_bench_cuda.cu:1522-1598) and hierarchize7
+ * (cu:1053-1160) kernels for timing next to this project's kernels.  TEST
+ * INFRASTRUCTURE ONLY: built by oracle/Makefile into oracle/_ref/ (never
+ * committed); no reference source is copied into this repository; REF_CU
+ * names the file it compiles.
  *
  * Build-level adjustments, none of which changes the kernel:
  *   - main() is renamed so the file links as a library;
@@ -21,10 +22,15 @@
  *     reference's constant tables (cu:17-18);
  *   - coordinates in [0, 1), so every cell index t = (int)(x 2^l) lies in
  *     its subspace.
- * The reference's hierarchization kernels are not exported: lane 0 of each
- * warp writes shared memory that the other lanes read with no __syncwarp
- * (hierarchize7, cu:1080-1097, cu:1100-1108, cu:1155-1156), a race whose
- * outcome can be an out-of-range index.
+ * hierarchize7 (cu:1053-1160) is compiled from the copy that
+ * patch_ref_cuda.py writes into _ref/: as it stands, lane 0 of each warp
+ * writes shared memory that the other lanes read with no __syncwarp
+ * (cu:1080-1097, cu:1100-1108, cu:1155-1156), a race whose outcome can be
+ * an out-of-range index; the copy adds the three warp barriers and nothing
+ * else.  Its launch condition, checked before any CUDA call: 6 <= n <= 10,
+ * so a finest-level subspace holds >= 32 points and every warp that reaches
+ * the barriers is whole (its lanes all pass `index < subspace_end`).
+ * The other hierarchization kernels (hierarchize0..6) are not exported.
  */
 #include <cuda_runtime.h>
 #include <stdlib.h>
@@ -122,5 +128,74 @@ done:
     cudaFree(d_trans);
     cudaFree(d_out);
     free(h_trans);
+    return e == cudaSuccess ? 0 : (int)e;
+}
+
+/* Hierarchizes the nodal values sg1d (N values, compact order) in place on
+ * the GPU with the reference's hierarchize7, launched as its main() does for
+ * h_opt 7 (cu:1790-1799: one launch per dimension, H_DP_MAT(d-1, n-1) CTAs of
+ * 256 threads, a device synchronize after each), `reps` times from the same
+ * nodal values; out gets the last run's surpluses.  ms_kernel: fastest time
+ * of the d launches; ms_total: fastest time of the reference's own timed
+ * region (the nodal values copied in, then the launches; cu:1713-1803).
+ * Returns 0, -1 for sizes outside the launch condition, -2 for a grid size
+ * mismatch, or a positive cudaError_t. */
+REFCUDA_API int refcuda_hierarchize7(int d, int n, const float *sg1d, int N, int reps, float *out,
+                                     float *ms_kernel, float *ms_total)
+{
+    int Nref = 0, S = 0, r, i;
+    float *d_sg1d = NULL;
+    cudaEvent_t t0 = NULL, k0 = NULL, k1 = NULL;
+    cudaError_t e = cudaSuccess;
+    if (d < 1 || d > MAX_NUM_DIMS || n < 6 || n > MAX_NUM_LEVELS || reps < 1) return -1;
+    memset(h_dp_mat, 0, sizeof(h_dp_mat)); /* init_dp_mat accumulates into it */
+    memset(h_lidx_vect, 0, sizeof(h_lidx_vect));
+    memset(h_par_lili, 0, sizeof(h_par_lili));
+    init_restr_vec(d, n);
+    init_dp_mat(d, n);
+    init_lidx_vect(d, n, &Nref, &S);
+    if (Nref != N) return -2;
+    init_par_lili(n);
+    const int num_levels = n; /* the name H_DP_MAT expects */
+    const int num_blocks = H_DP_MAT((d - 1), (n - 1)); /* subspaces of the finest level */
+    const int num_threads = 256;
+    const size_t smem = (size_t)(d + n + (d + 1)) * (num_threads / WARP_SIZE) * sizeof(int);
+#define CK(x)                            \
+    do {                                 \
+        e = (x);                         \
+        if (e != cudaSuccess) goto done; \
+    } while (0)
+    CK(cudaMemcpyToSymbol(d_dp_mat, h_dp_mat, d * n * sizeof(int)));
+    CK(cudaMemcpyToSymbol(d_lidx_vect, h_lidx_vect, n * sizeof(int)));
+    CK(cudaMemcpyToSymbol(d_par_lili, h_par_lili, 4 * ((1 << n) - 1) * sizeof(int)));
+    CK(cudaMalloc(&d_sg1d, (size_t)N * sizeof(float)));
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&k0));
+    CK(cudaEventCreate(&k1));
+    *ms_kernel = *ms_total = -1.0f;
+    for (r = 0; r < reps; r++) {
+        float tk = 0.0f, tt = 0.0f;
+        CK(cudaEventRecord(t0, 0));
+        CK(cudaMemcpy(d_sg1d, sg1d, (size_t)N * sizeof(float), cudaMemcpyHostToDevice));
+        CK(cudaEventRecord(k0, 0));
+        for (i = 0; i < d; ++i) {
+            hierarchize7<<<num_blocks, num_threads, smem>>>(d, n, d_sg1d, i);
+            CK(cudaGetLastError());
+            CK(cudaDeviceSynchronize());
+        }
+        CK(cudaEventRecord(k1, 0));
+        CK(cudaEventSynchronize(k1));
+        CK(cudaEventElapsedTime(&tk, k0, k1));
+        CK(cudaEventElapsedTime(&tt, t0, k1));
+        if (*ms_kernel < 0.0f || tk < *ms_kernel) *ms_kernel = tk;
+        if (*ms_total < 0.0f || tt < *ms_total) *ms_total = tt;
+    }
+    CK(cudaMemcpy(out, d_sg1d, (size_t)N * sizeof(float), cudaMemcpyDeviceToHost));
+#undef CK
+done:
+    if (t0) cudaEventDestroy(t0);
+    if (k0) cudaEventDestroy(k0);
+    if (k1) cudaEventDestroy(k1);
+    cudaFree(d_sg1d);
     return e == cudaSuccess ? 0 : (int)e;
 }

@@ -117,3 +117,8 @@ def test_reference_cuda_harness_refuses_unsafe_sizes():
     Y[3, 1] = 1.0
     with pytest.raises(RuntimeError, match="returned -1"):
         ReferenceCUDA.evaluate5(2, 4, surplus, Y, 32)
+    # hierarchize7: its warp barriers need whole warps, so n < 6 is refused;
+    # so are n > 10 and d > 20 (the constant tables' sizes)
+    for d, n in ((2, 4), (4, 5), (2, 11), (21, 6)):
+        with pytest.raises(RuntimeError, match="returned -1"):
+            ReferenceCUDA.hierarchize7(d, n, np.zeros(49, np.float32))
