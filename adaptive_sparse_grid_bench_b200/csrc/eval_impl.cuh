@@ -117,6 +117,13 @@ __device__ __forceinline__ void kahan_add(FV<P> &s, FV<P> &c, FV<P> v)
     s = t;
 }
 
+/* cell index at level l (0..15) from T = floor(x 2^15): T >> (15 - l).
+ * Level 0 has one cell and T < 2^15 for every x in [0,1) (x 2^15 is exact),
+ * so its index is 0; that is written out as a constant because the compiler
+ * cannot bound T, which comes from a float conversion, and would otherwise
+ * shift and multiply a zero in every row and plane of level 0. */
+__device__ __forceinline__ uint32_t cell_at(uint32_t T, int l) { return l == 0 ? 0u : T >> (kTB - l); }
+
 /* hat at the current level from the fractional part y = frac(x 2^l) */
 __device__ __forceinline__ float hat_of(float y) { return 1.0f - fabsf(fmaf(2.0f, y, -1.0f)); }
 
@@ -179,8 +186,8 @@ __device__ __forceinline__ void block2_fixed(const float *__restrict__ alpha, co
         const float *path[P]; /* the point's path: its L+1 surpluses of this row */
 #pragma unroll
         for (int p = 0; p < P; ++p)
-            path[p] = alpha + (base[p] + aoff_reg(r, a) + (in.TA[p] >> (kTB - a)) * plen_reg(r, a) +
-                               (in.TB[p] >> (kTB - L)) * (uint32_t)SG_PATH_WIDTH(L + 1));
+            path[p] = alpha + (base[p] + aoff_reg(r, a) + cell_at(in.TA[p], a) * plen_reg(r, a) +
+                               cell_at(in.TB[p], L) * (uint32_t)SG_PATH_WIDTH(L + 1));
         FV<P> sr = FV<P>::all(0.0f);
         /* slots 2j, 2j+1 in one 8-byte load (paths of L >= 1 start even) */
 #pragma unroll
@@ -215,7 +222,7 @@ __device__ __forceinline__ void block3_planes(const float *__restrict__ alpha, c
     uint32_t sb[P];
     FV<P> s2;
 #pragma unroll
-    for (int p = 0; p < P; ++p) sb[p] = base[p] + coff_reg(R, C) + (in.TC[p] >> (kTB - C)) * blk2_reg(R - C);
+    for (int p = 0; p < P; ++p) sb[p] = base[p] + coff_reg(R, C) + cell_at(in.TC[p], C) * blk2_reg(R - C);
     block2_fixed<R - C, P>(alpha, sb, in, s2);
     s = (C == 0) ? vmul(in.hC(0), s2) : vfma(in.hC(C), s2, s);
     if constexpr (C < R) block3_planes<R, C + 1, P>(alpha, base, in, s);
