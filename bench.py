@@ -57,9 +57,10 @@ EVAL_SRC = os.path.join(ROOT, "adaptive_sparse_grid_bench_b200", "csrc", "eval_i
 #   dram_bytes: dram__bytes_read.sum + dram__bytes_write.sum of one full
 #     2^24-point launch (one-pass metrics, so the full launch was captured);
 #   inst_per_pair: smsp__inst_executed.sum x 32 / (points x subspaces) of a
-#     262,144-point launch of the same grid.
-EVAL_CAPTURE = {"source_sha16": "0789b8dc88ff7494", "captured": "2026-12-04", "dram_bytes": 2.919e9 + 0.601e9,
-                "inst_per_pair": 8.10}
+#     1,048,576-point launch of the same grid (two points per thread, wide preset).
+#   (either may be None: not captured on this source)
+EVAL_CAPTURE = {"source_sha16": "ab15c4c8da0625a8", "captured": "2026-12-04", "dram_bytes": 2.953e9 + 0.588e9,
+                "inst_per_pair": None}
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
@@ -548,7 +549,7 @@ def run_b200(args, rank: int, world: int, local_rank: int, wl=None, extras: bool
                               f"no capture for evaluation source {src_sha}",
             "kernel": "k_evaluate", "peak_source": peak_src,
             "bytes": "4*(S+d+1) per query point (cache-served surplus reads counted)"}
-    if cap:
+    if cap and cap["inst_per_pair"]:
         # SM issue roofline: thread instructions per pair (ncu) x pairs/s
         # against 148 SMs x 4 schedulers x one warp instruction per clock
         mhz = clocks.get("sm_mhz") or float(peaks.get("sm_max_mhz", 1965.0))
