@@ -60,7 +60,7 @@ EVAL_SRC = os.path.join(ROOT, "adaptive_sparse_grid_bench_b200", "csrc", "eval_i
 #     1,048,576-point launch of the same grid (two points per thread, wide preset).
 #   (either may be None: not captured on this source)
 EVAL_CAPTURE = {"source_sha16": "ab15c4c8da0625a8", "captured": "2026-12-04", "dram_bytes": 2.953e9 + 0.588e9,
-                "inst_per_pair": None}
+                "inst_per_pair": 7.14}
 SM_COUNT, SCHEDULERS_PER_SM = 148, 4
 
 
