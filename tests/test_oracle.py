@@ -122,3 +122,31 @@ def test_reference_cuda_harness_refuses_unsafe_sizes():
     for d, n in ((2, 4), (4, 5), (2, 11), (21, 6)):
         with pytest.raises(RuntimeError, match="returned -1"):
             ReferenceCUDA.hierarchize7(d, n, np.zeros(49, np.float32))
+
+
+def test_ref_cuda_patch_rules():
+    # the warp-barrier patch of the reference's hierarchize7 (oracle/patch_ref_cuda.py),
+    # on a stand-in text with the kernel's three hand-over shapes: each rule must match
+    # exactly once inside hierarchize7, nothing outside it changes, and a missing shape
+    # stops the build instead of yielding an unpatched kernel
+    from oracle.patch_ref_cuda import patch
+    head = "__global__ void hierarchize6(int x) { if (0 == lane)\n  --levels[crt_dim]; }\n"
+    body = ("__global__ void hierarchize7(int x) {\n"
+            "  if (0 == lane) { levels[crt_dim] = saved_level; }\n"
+            "  for (; levels[crt_dim] >= 1; --crt_level) {\n"
+            "    if (0 == lane) {\n"
+            "      for (int l = d - 2; l >= 0; l--)\n"
+            "        prefix_sums[l] = prefix_sums[l + 1] + levels[l];\n"
+            "    }\n"
+            "    work();\n"
+            "    if (0 == lane)\n"
+            "      --levels[crt_dim];\n"
+            "  }\n}\n")
+    tail = "__global__ void evaluate5(int x) { }\n"
+    out = patch(head + body + tail)
+    assert out.startswith(head) and out.endswith(tail)
+    assert out.count("__syncwarp();") == 4
+    assert "__syncwarp(); for (; levels[crt_dim] >= 1;" in out
+    assert "__syncwarp(); if (0 == lane) --levels[crt_dim]; __syncwarp();" in out
+    with pytest.raises(SystemExit):
+        patch(head + body.replace("--levels[crt_dim];", "levels[crt_dim]--;") + tail)
